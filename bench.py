@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark of the monodomain time step (node-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tcb|reference]
+
+Workload (default ``ttp_cube``): ten Tusscher-Panfilov ENDO on a 100^3-cell
+tetrahedral cube (1,030,301 nodes, 6 M tets), see torchcor_b200/workloads.py.
+A step is one monodomain time step: ionic update + stimulus + LAT/RT,
+right-hand side, Jacobi-PCG to atol = rtol = 1e-5.
+
+``--impl tcb`` (default): K steps timed with CUDA events on the launch stream
+after W warm-up steps, barrier + synchronize on both sides, max over ranks;
+each rank runs an independent replica (the reference has no domain
+decomposition: "replicas only").  Prints one JSON line with value (node-steps/s,
+whole job), e2e (one full solve through the public API from host arrays),
+roofline (CG kernel, algorithmic bytes / event time vs measured HBM peak),
+clocks and the CPU baseline (the oracle on the same workload, host cores).
+
+``--impl reference``: rank 0 times the oracle (CPU restatement of the
+reference path, torch CPU with every host thread) on the same workload:
+assembly untimed, then a bounded number of steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "node-steps/s"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(impl):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and impl == "tcb":
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def make_sim(wl, device, T=None):
+    from torchcor_b200.ionic import CourtemancheRamirezNattel, ModifiedMS2v, TenTusscherPanfilov
+    from torchcor_b200.simulator import Monodomain
+    if wl.model == "ttp":
+        im = TenTusscherPanfilov(wl.cell_type, wl.dt, device=device)
+    elif wl.model == "crn":
+        im = CourtemancheRamirezNattel(wl.dt, device=device)
+    else:
+        im = ModifiedMS2v(wl.dt, device=device)
+    sim = Monodomain(im, T=wl.T if T is None else T, dt=wl.dt, device=device)
+    sim.load_arrays(wl.nodes_mm, wl.elems, wl.regions, wl.fibres)
+    for c in wl.conductivity:
+        sim.add_conductivity(**c)
+    for s in wl.stimuli:
+        sim.add_stimulus(None, s["start"], s["duration"], s["intensity"], period=wl.T, region=s["region"])
+    return sim
+
+
+def oracle_sim(wl):
+    from oracle import port as P
+    if wl.model == "ttp":
+        im = P.TenTusscherPanfilov(wl.cell_type, wl.dt)
+    elif wl.model == "crn":
+        im = P.CourtemancheRamirezNattel(wl.dt)
+    else:
+        im = P.ModifiedMS2v(wl.dt)
+    sim = P.Monodomain(im, wl.T, wl.dt)
+    sim.load_arrays(wl.nodes_mm, wl.elems, wl.regions, wl.fibres)
+    for c in wl.conductivity:
+        sim.add_conductivity(**c)
+    for s in wl.stimuli:
+        sim.add_stimulus(torch.from_numpy(np.asarray(s["region"])), s["start"], s["duration"], s["intensity"], wl.T)
+    return sim
+
+
+def time_oracle(wl, budget_s, min_steps=2, max_steps=None):
+    """Oracle on the workload: assembly (timed separately), then steps until
+    ``budget_s`` seconds of stepping (at least ``min_steps``)."""
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    sim = oracle_sim(wl)
+    t0 = time.perf_counter()
+    sim.assemble()
+    t_asm = time.perf_counter() - t0
+    u = sim.ionic.initialize(sim.n_nodes)
+    sim.cg.initialize(u, linear_guess=True)
+    t = 0.0
+    n = 0
+    el = 0.0
+    while (el < budget_s or n < min_steps) and (max_steps is None or n < max_steps) and n < wl.nt:
+        t += wl.dt
+        t1 = time.perf_counter()
+        u, _ = sim.step(u, t, 1e-5, 1e-5, 100)
+        el += time.perf_counter() - t1
+        n += 1
+    return dict(value=wl.n_nodes * n / el, steps=n, seconds=el, assemble_s=t_asm, cores=cores)
+
+
+def reference_arm(a, wl, world, rank):
+    if rank != 0:
+        return
+    # warm-up steps are run untimed inside the same oracle session; the timed
+    # sample is bounded to keep the whole run within a few minutes
+    budget = float(os.environ.get("TCB_REFERENCE_BUDGET_S", "60"))
+    r = time_oracle(wl, budget_s=budget, min_steps=min(a.steps, 3), max_steps=a.steps)
+    v = r["value"]
+    sample = (f"oracle (CPU restatement of the reference path, torch CPU, {r['cores']} threads) on the full "
+              f"workload: assembly {r['assemble_s']:.1f} s untimed, then {r['steps']} timed steps "
+              f"({r['seconds']:.1f} s)")
+    line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world, "steps": r["steps"], "warmup": 0,
+            "ms_per_step": 1000 * r["seconds"] / r["steps"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": wl.name, "nodes": wl.n_nodes, "elements": int(len(wl.elems)), "dt_ms": wl.dt,
+                       "T_ms": wl.T, "parallelism": "replicas only"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": r["cores"], "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def tcb_arm(a, wl, world, rank, local):
+    from torchcor_b200 import _lib
+    from torchcor_b200.workloads import algorithmic_bytes
+    import ctypes as C
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    need = a.warmup + a.steps + a.profile_steps
+    T_run = max(wl.T, (need + 1) * wl.dt)
+    sim = make_sim(wl, dev, T=T_run)
+    sim.assemble()
+    sys_ = sim.system
+    sim._setup(1e-5, 1e-5, 100, True, True, 1.0, keep_snapshots=False)
+    stream = torch.cuda.current_stream(dev)
+    sim.run_steps(a.warmup)
+    torch.cuda.synchronize(dev)
+    lib = _lib.load()
+    _lib.check(lib.tcb_mono_check(C.byref(sim._sim["struct"]), stream.cuda_stream))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        sim.run_steps(a.steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        torch.distributed.barrier()
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    _lib.check(lib.tcb_mono_check(C.byref(sim._sim["struct"]), stream.cuda_stream))
+    iters = sim._sim["step_iters"][a.warmup + 1: a.warmup + a.steps + 1].sum().item()
+    k_loop = iters / a.steps + 1.0                    # CG loop passes per step (n_iter + 1)
+    # per-kernel event times for the roofline (separate pass, same stream)
+    msi, msc = C.c_double(0.0), C.c_double(0.0)
+    s0 = sim._sim["next_step"]
+    _lib.check(lib.tcb_mono_profile(C.byref(sim._sim["struct"]), s0, s0 + a.profile_steps, stream.cuda_stream,
+                                    C.byref(msi), C.byref(msc)))
+    sim._sim["next_step"] = s0 + a.profile_steps
+    p_iters = sim._sim["step_iters"][s0: s0 + a.profile_steps].sum().item()
+    kp = p_iters / a.profile_steps + 1.0
+    b_ion, b_rhs, b_iter = algorithmic_bytes(sys_.n, sys_.nnz, sim.ionic_model.state.shape[0])
+    t_ion = msi.value / a.profile_steps * 1e-3
+    t_cg = msc.value / a.profile_steps * 1e-3
+    peak, peak_kind = peaks()
+    cg_bytes = b_rhs + kp * b_iter
+    gbs_cg = cg_bytes / t_cg / 1e9
+    gbs_ion = b_ion / t_ion / 1e9
+    step_bytes = b_ion + b_rhs + k_loop * b_iter
+    value = world * wl.n_nodes * a.steps / (ms / 1e3)
+    dominant = ("cg_kernel", gbs_cg, cg_bytes) if t_cg >= t_ion else ("mono_ionic_kernel", gbs_ion, b_ion)
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(dominant[0])
+    del sim
+    torch.cuda.empty_cache()
+
+    # e2e: one full solve of the workload through the public API from host arrays
+    e2e = None
+    if not a.no_e2e:
+        if world > 1:
+            torch.distributed.barrier()
+        with tempfile.TemporaryDirectory() as d:
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            sim2 = make_sim(wl, dev)
+            sim2.solve(1e-5, 1e-5, 100, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1.0,
+                       verbose=False, result_path=d)
+            torch.cuda.synchronize(dev)
+            wall = time.perf_counter() - t0
+            h2d = (wl.nodes_mm.size * 4 + wl.elems.size * 4 + wl.regions.size * 4 + wl.fibres.size * 4 +
+                   wl.n_nodes * 4 + (wl.nt + 1) * 8)
+            d2h = 2 * wl.n_nodes * 4 + (wl.nt // int(1.0 / wl.dt) + 1) * wl.n_nodes * 4 + (wl.nt + 1) * 4
+            del sim2
+        if world > 1:
+            t = torch.tensor([wall], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": world * wl.n_nodes * wl.nt / wall, "unit": METRIC,
+               "h2d_bytes_per_step": int(h2d // wl.nt), "d2h_bytes_per_step": int(d2h // wl.nt),
+               "what": f"one Monodomain.solve of the workload (T={wl.T} ms, {wl.nt} steps) from host arrays: "
+                       f"mesh upload, assembly, all steps, AT/RT/Vm download and save; wall {wall:.2f} s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        r = time_oracle(wl, budget_s=float(os.environ.get("TCB_CPU_BASELINE_S", "15")), min_steps=3)
+        cpu = {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": "port",
+               "sample": f"oracle on the full workload, {r['steps']} steps after an untimed "
+                         f"{r['assemble_s']:.1f} s assembly ({r['seconds']:.1f} s of stepping)"}
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "nodes": wl.n_nodes, "elements": int(len(wl.elems)), "nnz": sys_.nnz,
+                   "dt_ms": wl.dt, "T_ms": wl.T, "parallelism": "replicas only" if world > 1 else "single",
+                   "cg_tol": 1e-5, "cg_iterations_per_step": iters / a.steps,
+                   "l2": "inputs larger than L2 (per-step working set > 300 MB)",
+                   "simulated_ms_per_s": world * wl.dt * a.steps / (ms / 1e3)},
+        "gpu_launches": 2 * a.steps,
+        "clocks": clk.summary(),
+        "roofline": {"bound": "hbm", "kernel": dominant[0], "achieved": dominant[1], "peak": peak,
+                     "unit": "GB/s", "frac": dominant[1] / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} HBM copy bandwidth",
+                     "kernels": {"cg_kernel": {"ms_per_launch": 1e3 * t_cg, "bytes": cg_bytes, "GB/s": gbs_cg,
+                                               "cg_loop_passes": kp},
+                                 "mono_ionic_kernel": {"ms_per_launch": 1e3 * t_ion, "bytes": b_ion,
+                                                       "GB/s": gbs_ion}},
+                     "step": {"bytes": step_bytes, "GB/s": step_bytes / (ms / a.steps * 1e-3) / 1e9}},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="tcb", choices=["tcb", "reference"])
+    ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube"])
+    ap.add_argument("--profile-steps", type=int, default=200)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    from torchcor_b200.workloads import WORKLOADS
+    world, rank, local = dist_setup(a.impl)
+    wl = WORKLOADS[a.workload]()
+    if a.impl == "reference":
+        reference_arm(a, wl, world, rank)
+        return
+    tcb_arm(a, wl, world, rank, local)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,178 @@
+/*
+ * tcb200.h - C ABI of libtcb200.so, the B200 (sm_100a) kernels behind the
+ * torchcor_b200 package: TorchCor's monodomain time step (ionic update with
+ * stimulus injection and activation/repolarisation tracking, P1 assembly into
+ * CSR, Jacobi-preconditioned CG).
+ *
+ * Conventions
+ *  - Every entry point returns an int status: TCB_OK (0) or a negative
+ *    TCB_E* code; tcb_status_string() names it and tcb_last_error() returns
+ *    the message of the last failure on the calling thread.
+ *  - Device pointers are plain pointers to memory the caller allocated (the
+ *    Python layer uses torch tensors); the library never frees caller memory.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *  - Per-node arrays have `n_pad` entries (n_nodes rounded up to 128); the
+ *    sparse matrices are stored as CSR (patterns bit-identical to the
+ *    reference's coalesced COO -> CSR) and, for the solver, as sliced ELL with
+ *    slice height 32 (TCB_SLICE) sharing one column array.
+ *
+ * Each declaration names the reference (TorchCor 0.1.8) interface it replaces.
+ */
+#ifndef TCB200_H
+#define TCB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCB_OK 0
+#define TCB_EINVAL (-1)     /* invalid argument (size, pointer, model id) */
+#define TCB_ECUDA (-2)      /* a CUDA runtime call failed */
+#define TCB_ETIMEOUT (-3)   /* a bounded device-side wait gave up */
+#define TCB_ENOMEM (-4)     /* host allocation failed */
+#define TCB_ERANGE (-5)     /* size beyond a stated limit */
+
+#define TCB_SLICE 32        /* sliced-ELL slice height (one warp) */
+#define TCB_MAX_STIMULI 32  /* stimuli per simulation (one bit each) */
+
+/* ionic model ids */
+#define TCB_MODEL_MS 1      /* ModifiedMS2v / MitchellSchaeffer (dimensional, mV) */
+#define TCB_MODEL_TTP 2     /* TenTusscherPanfilov */
+#define TCB_MODEL_CRN 3     /* CourtemancheRamirezNattel */
+
+int tcb_version(void);
+const char* tcb_status_string(int status);
+/* Copies the last error message of this thread into buf (truncated). */
+int tcb_last_error(char* buf, int64_t len);
+
+/* ---------------------------------------------------------------- pattern
+ * CSR pattern of the assembled P1 operator plus a deterministic scatter map.
+ * Replaces the Python-list COO build + coalesce of
+ * torchcor/core/assemble.py:217-248 (tets) and :67-96 (triangles): the CSR
+ * (rowptr, col) equals coalesce(COO).to_sparse_csr() of the reference; each
+ * slot's contributions are listed in the reference's COO order
+ * ((a*k+b)*E + e ascending), as flat indices e*k*k + a*k + b into the
+ * (E, k, k) local-matrix array.  Host code (elems in host memory).
+ */
+int tcb_pattern_size(const int32_t* elems, int64_t n_elems, int32_t k, int64_t n_nodes, int64_t* nnz);
+int tcb_pattern_build(const int32_t* elems, int64_t n_elems, int32_t k, int64_t n_nodes,
+                      int32_t* rowptr /* n_nodes+1 */, int32_t* col /* nnz */,
+                      int32_t* slot_ptr /* nnz+1 */, int32_t* slot_src /* k*k*n_elems */,
+                      int32_t* diag /* n_nodes: slot of (i,i) */);
+/* Sliced-ELL layout of a CSR pattern: slice_ptr[n_slices+1] entry offsets
+ * (each slice holds 32 * its widest row entries).  Host code. */
+int tcb_sell_layout(const int32_t* rowptr, int64_t n_rows, int64_t* slice_ptr, int64_t* n_entries);
+
+/* ---------------------------------------------------------------- assembly
+ * Element matrices of P1 tetrahedra (k=4) or surface triangles (k=3).
+ * Replaces Matrices3D.construct_local_matrices (assemble.py:202-215) and
+ * Matrices3DSurface (assemble.py:99-145), with the conductivity tensor of
+ * Conductivity.calculate_sigma (conductivity.py:64-67) formed in the kernel:
+ * sigma = st*I + (sl-st) f f^T per element.
+ * Outputs: ke[E*k*k] stiffness, mw[E] = volume/20 (tets) or area/12 (tris).
+ */
+int tcb_assemble_local(int32_t k, const float* nodes /* N*3, mm */, const int32_t* elems, int64_t n_elems,
+                       const float* sl, const float* st, const float* fibres /* E*3 */,
+                       float* ke, float* mw, void* stream);
+/* Sum element contributions into CSR values in the scatter map's order
+ * (replaces the coalesce of assemble.py:233-248). m_val gets mw*pattern. */
+int tcb_assemble_gather(int32_t k, const int32_t* slot_ptr, const int32_t* slot_src, int64_t nnz,
+                        const float* ke, const float* mw, float* k_val, float* m_val, void* stream);
+/* Monodomain.assemble system values (monodomain.py:93-106, preconditioner.py:9-27):
+ * k_val /= chi (in place); a_val = m*cm + (k*dt)*theta; k_rhs = ((1-theta)*dt)*k;
+ * d_inv[i] = 1/a(i,i) (0 for i >= n_nodes up to n_pad). */
+int tcb_assemble_system(int64_t nnz, int64_t n_nodes, int64_t n_pad, const int32_t* diag, float* k_val,
+                        const float* m_val, double chi, double cm, double dt, double theta,
+                        float* a_val, float* k_rhs, float* d_inv, void* stream);
+/* Repack up to 4 CSR value arrays (and the columns) into sliced ELL; padding
+ * entries get column = own row and value 0. */
+int tcb_sell_pack(int64_t n_rows, const int32_t* rowptr, const int32_t* col, const int64_t* slice_ptr,
+                  int64_t n_slices, int32_t n_vals, const float* const* vals /* host array of device ptrs */,
+                  int32_t* sell_col, float* const* sell_vals, void* stream);
+
+/* ---------------------------------------------------------------- ionic
+ * Ionic models.  `params` is a host array of doubles in the order of
+ * tcb_model_params(model) (the Python-level attributes of the reference
+ * class, plus dt); state is (n_states x n_pad) structure-of-arrays.
+ * Replaces ModifiedMS2v (ionic/ModifiedMS2v.py:4-44), TenTusscherPanfilov
+ * (ionic/TenTusscherPanfilov.py:6-454), CourtemancheRamirezNattel
+ * (ionic/CourtemancheRamirezNattel.py:5-444).
+ */
+const char* tcb_model_params(int32_t model);       /* comma-separated parameter names */
+const char* tcb_model_states(int32_t model);       /* comma-separated state names (row order) */
+int tcb_model_layout(int32_t model, const double* params, int64_t* n_states, int64_t* table_floats);
+/* construct_tables (TTP :197-318, CRN :212-328); no-op for MS */
+int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream);
+/* initialize(n_nodes): fill state rows and V with the initial values */
+int tcb_model_init(int32_t model, const double* params, float* state, int64_t n_pad, float* v, void* stream);
+/* differentiate(V): dv = -Iion and the state update, for n nodes */
+int tcb_model_differentiate(int32_t model, const double* params, const float* tables, float* state,
+                            int64_t n_pad, int64_t n, const float* v, float* dv, void* stream);
+
+/* ---------------------------------------------------------------- time loop
+ * One simulation on the device.  Replaces Monodomain.step / solve's loop
+ * (monodomain.py:109-196) with ConjugateGradient.solve (solver.py:40-76).
+ * Step n (1-based) reads the membrane potential ring x[(n-1)%3] (solution of
+ * step n-1) and x[(n+1)%3] (the one before) and writes x[n%3].
+ */
+typedef struct tcb_mono {
+    int64_t n_nodes, n_pad, n_slices, nt;
+    int32_t model, n_states;
+    /* matrix (sliced ELL, TCB_SLICE rows per slice) */
+    const int64_t* slice_ptr;
+    const int32_t* col;
+    const float* m_val;      /* M */
+    const float* k_val;      /* ((1-theta)*dt) * K/chi */
+    const float* a_val;      /* Cm*M + theta*dt*K/chi */
+    const float* d_inv;      /* 1/diag(A) */
+    /* ionic */
+    float* state;
+    const float* tables;
+    /* vectors (n_pad each; x is 3*n_pad) */
+    float* x;
+    float* bprime;
+    float* r;
+    float* p;
+    float* ap;
+    float* at;
+    float* rt;
+    float* snapshots;        /* row j = solution of step j*per_frame, n_nodes per row; may be NULL */
+    /* stimuli and schedule */
+    const uint32_t* stim_bits;   /* per node: bit s set if the node is in stimulus s */
+    const float* step_t;         /* [nt+1]: fp32 of the accumulated time t_n */
+    const uint32_t* step_stim;   /* [nt+1]: bit s set if stimulus s is on at step n */
+    float stim_amp[TCB_MAX_STIMULI];
+    /* solver */
+    double a_tol, r_tol;
+    int32_t max_iter, linear_guess, at_rt, per_frame;
+    float cm, dt;
+    /* device bookkeeping (caller-allocated, zero-initialised) */
+    int32_t* step_iters;     /* [nt+1] CG iterations of each step */
+    int32_t* counter;        /* [4]: next step, error code, 2 spare */
+    double* scratch;         /* >= tcb_mono_scratch_doubles() */
+    uint32_t* barrier;       /* [4] grid-barrier words */
+    /* model parameters (host) */
+    const double* params;
+} tcb_mono;
+
+int64_t tcb_mono_scratch_doubles(void);
+/* Run steps [step_begin, step_end) (1-based, step_begin must equal the device
+ * counter).  Non-convergence is not an error (n_iter == max_iter), as in the
+ * reference. */
+int tcb_mono_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream);
+/* Like tcb_mono_run, recording CUDA events around every kernel on `stream`;
+ * adds the summed device times (ms) of the ionic and CG kernels to
+ * ms_ionic / ms_cg (for roofline accounting; costs one event pair per launch). */
+int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream, double* ms_ionic,
+                     double* ms_cg);
+/* Activation/repolarisation update and snapshot for the final step. */
+int tcb_mono_finish(const tcb_mono* m, void* stream);
+/* Device error word after a run (TCB_OK or TCB_ETIMEOUT); synchronises the stream. */
+int tcb_mono_check(const tcb_mono* m, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

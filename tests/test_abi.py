@@ -1,0 +1,203 @@
+"""The C ABI of libtcb200.so and the host-side logic that needs no GPU."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from tests.golden import cases as CS
+from tests.helpers import golden
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "tcb200.h"
+
+
+def declared_functions():
+    src = HEADER.read_text()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tcb_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len(names) >= 18
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_python_signatures_cover_header(lib):
+    from torchcor_b200 import _lib
+    assert sorted(n for n, _, _ in _lib.SIGNATURES) == declared_functions()
+
+
+def test_status_strings(lib):
+    assert lib.tcb_version() >= 1
+    assert lib.tcb_status_string(0) == b"ok"
+    assert lib.tcb_status_string(-3) == b"device wait timed out"
+
+
+def test_struct_layout_matches_header(lib):
+    from torchcor_b200 import _lib
+    # the ctypes mirror must be as large as the C struct the library reads
+    src = HEADER.read_text()
+    body = src[src.index("typedef struct tcb_mono"):src.index("} tcb_mono;")]
+    fields = re.findall(r"\b([a-z_]+)\s*(?:\[[A-Z_]+\])?\s*[;,]", body)
+    names = [f for f, *_ in _lib.tcb_mono._fields_]
+    for f in names:
+        assert f in body, f
+    assert C.sizeof(_lib.tcb_mono) % 8 == 0
+
+
+@pytest.mark.parametrize("model,cls", [(1, "ModifiedMS2v"), (2, "TenTusscherPanfilov"),
+                                       (3, "CourtemancheRamirezNattel")])
+def test_model_parameter_names_resolve(lib, model, cls):
+    from torchcor_b200 import _lib, ionic
+    m = getattr(ionic, cls)(*(("ENDO", 0.01) if model == 2 else (0.01,)), device="cpu")
+    p = m.param_array()
+    assert len(p) == len(_lib.model_params(model))
+    assert np.isfinite(p).all()
+    ns = C.c_int64()
+    nt = C.c_int64()
+    assert lib.tcb_model_layout(model, p.ctypes.data, C.byref(ns), C.byref(nt)) == 0
+    assert ns.value == len(_lib.model_states(model))
+
+
+def test_table_sizes_match_reference_arange(lib):
+    from torchcor_b200 import ionic
+    ns, nt = C.c_int64(), C.c_int64()
+    m = ionic.TenTusscherPanfilov("ENDO", 0.01, device="cpu")
+    lib.tcb_model_layout(2, m.param_array().ctypes.data, C.byref(ns), C.byref(nt))
+    rows = lambda a, b, r: torch.arange(a, b, r).shape[0]  # noqa: E731
+    assert nt.value == rows(-800., 800., 0.05) * 27 + rows(0.00001, 10.0, 0.00001) * 3 + rows(-800., 800., 0.05)
+    m = ionic.CourtemancheRamirezNattel(0.02, device="cpu")
+    lib.tcb_model_layout(3, m.param_array().ctypes.data, C.byref(ns), C.byref(nt))
+    assert nt.value == rows(-200., 200., 0.1) * 32 + rows(3e-4, 30.0, 3e-4) * 5 + rows(-2e-11, 10.0e-11, 2e-15) * 3
+
+
+@pytest.mark.parametrize("name", ["cube6_ms_f32", "cfg1_ms_f32", "cube8_ttp_f32", "ico3_crn_f32",
+                                  "cube4_ms_period_f32"])
+def test_pattern_bit_exact(lib, name):
+    from torchcor_b200.core.assemble import build_pattern
+    case = CS.case(name)
+    g = golden(name)
+    nodes, elems, _, _ = CS.mesh_arrays(case)
+    p = build_pattern(elems, len(nodes))
+    assert np.array_equal(p.rowptr, g["crow"])
+    assert np.array_equal(p.col, g["col"])
+    assert np.array_equal(p.col[p.diag], np.arange(len(nodes)))
+    # every element contribution is listed exactly once, in reference COO order per slot
+    k = elems.shape[1]
+    assert p.slot_ptr[-1] == k * k * len(elems)
+    assert np.array_equal(np.sort(p.slot_src), np.arange(k * k * len(elems)))
+    E = len(elems)
+    src = p.slot_src.astype(np.int64)
+    order = ((src % (k * k)) * E + src // (k * k))
+    seg = np.repeat(np.arange(p.nnz), np.diff(p.slot_ptr))
+    same = seg[1:] == seg[:-1]
+    assert (order[1:][same] > order[:-1][same]).all()
+    # the listed element entry really lands in that slot
+    e, ab = src // (k * k), src % (k * k)
+    rows = elems[e, ab // k]
+    cols = elems[e, ab % k]
+    slot_row = np.repeat(np.arange(len(nodes)), np.diff(p.rowptr))[seg]
+    assert np.array_equal(rows, slot_row) and np.array_equal(cols, p.col[seg])
+
+
+def test_pattern_cube_formula(lib):
+    from torchcor_b200 import meshgen
+    from torchcor_b200.core.assemble import build_pattern
+    for n in (3, 7, 12):
+        nodes, elems = meshgen.cube(n, 1.0)
+        p = build_pattern(elems, len(nodes))
+        assert p.nnz == (n + 1) ** 3 + 2 * (3 * n * (n + 1) ** 2 + 3 * n ** 2 * (n + 1) + n ** 3)
+
+
+def test_pattern_rejects_bad_input(lib):
+    from torchcor_b200._lib import TcbError
+    from torchcor_b200.core.assemble import build_pattern
+    with pytest.raises(TcbError):
+        build_pattern(np.array([[0, 1, 2, 9]]), 4)        # node index out of range
+    with pytest.raises(TcbError):
+        build_pattern(np.array([[0, 1, 2, 3]]), 6)        # nodes 4, 5 belong to no element
+
+
+def test_sell_layout(lib):
+    rowptr = np.array([0, 3, 5, 9] + [9 + 2 * i for i in range(1, 40)], dtype=np.int32)
+    n = len(rowptr) - 1
+    sp = np.empty((n + 31) // 32 + 1, dtype=np.int64)
+    ne = C.c_int64()
+    assert lib.tcb_sell_layout(rowptr.ctypes.data, n, sp.ctypes.data, C.byref(ne)) == 0
+    lens = np.diff(rowptr)
+    for s in range(len(sp) - 1):
+        assert sp[s + 1] - sp[s] == 32 * lens[32 * s: 32 * s + 32].max()
+    assert ne.value == sp[-1]
+
+
+def test_stimulus_schedule_matches_oracle():
+    from oracle import port as P
+    from torchcor_b200.core.stimulation import Stimuli
+    dt, T = 0.01, 12.0
+    nt = int(T / dt)
+    specs = [(0.0, 1.0, 100, 4.0, 2), (5.0, 1.0, 50, T, 1), (0.3, 0.01, 10, 0.7, 5)]
+    ours = Stimuli(10, "cpu", torch.float32)
+    ref = P.Stimuli(10, torch.float32)
+    for k, (a, d, I, per, cnt) in enumerate(specs):
+        ours.add(None, a, d, I, per, cnt, region=[k])
+        ref.add(torch.tensor([k]), a, d, I, per, cnt)
+    t32, mask = ours.schedule(nt, dt)
+    t = 0
+    for n in range(1, nt + 1):
+        t += dt
+        want = sum(1 << k for k, s in enumerate(ref.items) if ref.active(s, t))
+        assert mask[n] == want, n
+        assert t32[n] == np.float32(t)
+        dense = ref.apply(t)
+        bits = ours.membership_bits() & mask[n]
+        amp = ours.amplitudes()
+        got = np.array([sum(amp[k] for k in range(3) if (b >> k) & 1) for b in bits], dtype=np.float32)
+        np.testing.assert_array_equal(got, dense.numpy())
+
+
+def test_mesh_reader_matches_oracle(tmp_path):
+    from oracle import port as P
+    from torchcor_b200.core.mesh import MeshReader
+    for name in ("cube6_ms_f32", "ico3_crn_f32"):
+        case = CS.case(name)
+        CS.write_case_mesh(case, tmp_path / name)
+        a = MeshReader(tmp_path / name).read(1000)
+        b = P.read_mesh(tmp_path / name, 1000)
+        for x, y in zip(a, b):
+            assert x.shape == y.shape and np.array_equal(x, y)
+
+
+def test_mesh_reader_count_mismatch(tmp_path):
+    from torchcor_b200.core.mesh import MeshReader
+    d = tmp_path / "bad"
+    d.mkdir()
+    (d / "m.pts").write_text("3\n0 0 0\n1 0 0\n")
+    (d / "m.elem").write_text("1\nTr 0 1 2 1\n")
+    (d / "m.lon").write_text("1\n1 0 0\n")
+    with pytest.raises(ValueError):
+        MeshReader(d).read()
+
+
+def test_conductivity_matches_oracle():
+    from oracle import port as P
+    from torchcor_b200.core.conductivity import Conductivity
+    reg = torch.tensor([1, 2, 2, 3, 1], dtype=torch.int32)
+    fib = torch.nn.functional.normalize(torch.rand(5, 3, dtype=torch.float64), dim=1).float()
+    for args in ([([1, 3], 0.5, 0.2), ([2], 0.9, 0.3)], [([1, 2, 3], 0.17, 0.019, 0.62, 0.2)]):
+        a, b = Conductivity(reg, torch.float32), P.Conductivity(reg, torch.float32)
+        for x in args:
+            a.add(*x)
+            b.add(*x)
+        for u, v in zip(a.calculate_sigma(fib), b.sigma(fib)):
+            assert (u is None and v is None) or torch.equal(u, v)
+
+
+def test_monodomain_requires_cuda():
+    from torchcor_b200.ionic import ModifiedMS2v
+    from torchcor_b200.simulator import Monodomain
+    with pytest.raises(RuntimeError):
+        Monodomain(ModifiedMS2v(0.01, device="cpu"), T=1.0, dt=0.01, device="cpu")

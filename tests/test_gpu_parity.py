@@ -1,0 +1,193 @@
+"""Parity of the sm_100a kernels with the oracle and the reference goldens.
+
+Tolerances: membrane potential within 1e-3 of the
+reference's range (max |dVm| <= 1e-3 * max |Vm_ref|), activation and
+repolarisation times within one dt, CSR pattern bit-exact.  Element-wise
+ionic arithmetic follows the reference's float32 operation order, so the
+remaining differences come from exp/log/expm1 implementations (a few ulp).
+"""
+import numpy as np
+import pytest
+import torch
+
+from tests.golden import cases as C
+from tests.helpers import case_mesh_dir, device_ionic, golden, oracle_ionic, run_device_tissue, run_oracle_tissue
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+# ------------------------------------------------------------------ tables
+@pytest.mark.parametrize("model,kw", [("ttp", dict(cell_type="ENDO", dt=0.01)), ("ttp", dict(cell_type="EPI", dt=0.02)),
+                                      ("crn", dict(dt=0.02)), ("crn", dict(dt=0.01))])
+def test_lookup_tables(lib, cuda, model, kw):
+    case = dict(model=model, dtype="f32", **kw)
+    ref = oracle_ionic(case)
+    ref.construct_tables()
+    dev = device_ionic(case, cuda)
+    dev.initialize(16)
+    t = dev.tables.cpu().numpy()
+    if model == "ttp":
+        parts = [ref.V_tab, ref.CaSS_tab, ref.VEk_tab]
+    else:
+        parts = [ref.V_tab, ref.Cai_tab, ref.fn_tab]
+    off = 0
+    for p in parts:
+        p = p.numpy()
+        got = t[off:off + p.size].reshape(p.shape)
+        off += p.size
+        # grid points differ from torch.arange's vectorised float32 grid by <= 1 ulp
+        np.testing.assert_allclose(got, p, rtol=2e-4, atol=1e-6 * np.abs(p).max(axis=0) + 1e-30)
+    assert off == t.size
+
+
+# ------------------------------------------------------------------ one differentiate() call
+@pytest.mark.parametrize("name", ["step_ms_f32", "step_ttp_f32", "step_ttp_epi_f32", "step_crn_f32"])
+def test_single_step(lib, cuda, name):
+    case = C.case(name)
+    g = golden(name)
+    im = device_ionic(case, cuda)
+    V0, st0 = C.random_ionic_inputs(case)
+    im.initialize(len(V0))
+    for k, v in st0.items():
+        setattr(im, k, torch.from_numpy(v))
+    dV = im.differentiate(torch.from_numpy(V0).to(cuda)).cpu().numpy()
+    ref = g["dV"]
+    scale = np.abs(ref) + 1e-3 * np.abs(ref).max()
+    assert (np.abs(dV - ref) <= 1e-4 * scale).mean() > 0.999
+    assert rel_err(dV, ref) < 1e-4
+    for k in st0:
+        np.testing.assert_allclose(getattr(im, k).cpu().numpy(), g["out_" + k], rtol=1e-4,
+                                   atol=1e-6 * np.abs(g["out_" + k]).max())
+
+
+# ------------------------------------------------------------------ single cell
+@pytest.mark.parametrize("name", ["cell_ms_f32", "cell_ttp_f32", "cell_crn_f32"])
+def test_single_cell_trace(lib, cuda, name):
+    case = C.case(name)
+    g = golden(name)
+    im = device_ionic(case, cuda)
+    V = im.initialize(1)
+    dt = case["dt"]
+    every = int(round(case["every"] / dt))
+    trace = []
+    t = 0.0
+    for n in range(int(case["T"] / dt)):
+        if n % every == 0:
+            trace.append(V.item())
+        V = V + dt * im.differentiate(V)
+        t += dt
+        if case["stim_start"] <= t <= case["stim_start"] + case["stim_dur"]:
+            V = V + dt * case["stim"]
+    trace = np.asarray(trace)
+    ref = g["trace"]
+    assert np.abs(trace - ref).max() <= 1e-3 * np.abs(ref).max(), np.abs(trace - ref).max()
+
+
+# ------------------------------------------------------------------ assembly
+@pytest.mark.parametrize("name", ["cube6_ms_f32", "cube8_ttp_f32", "ico3_crn_f32", "cube4_ms_period_f32"])
+def test_assembly_matches_reference(lib, cuda, name, tmp_path):
+    from torchcor_b200.ionic import ModifiedMS2v
+    from torchcor_b200.simulator import Monodomain
+    case = C.case(name)
+    g = golden(name)
+    sim = Monodomain(ModifiedMS2v(case["dt"], device=cuda), T=case["T"], dt=case["dt"], device=cuda)
+    sim.load_mesh(case_mesh_dir(case, tmp_path))
+    for c in case["conductivity"]:
+        sim.add_conductivity(**c)
+    s = sim.assemble()
+    assert np.array_equal(s.rowptr.cpu().numpy(), g["crow"])
+    assert np.array_equal(s.col.cpu().numpy(), g["col"])
+    # float64 element matrices rounded once vs the reference's float32 LU: a few ulp
+    np.testing.assert_allclose(s.m_val.cpu().numpy(), g["M"], rtol=2e-6)
+    K = g["K"]
+    np.testing.assert_allclose(s.k_val.cpu().numpy(), K, rtol=1e-4, atol=2e-6 * np.abs(K).max())
+    A = g["A"]
+    np.testing.assert_allclose(s.a_val.cpu().numpy(), A, rtol=1e-4, atol=2e-6 * np.abs(A).max())
+    np.testing.assert_allclose(s.d_inv[: s.n].cpu().numpy(), g["PC"], rtol=1e-5)
+    assert (s.d_inv[s.n:] == 0).all()
+
+
+# ------------------------------------------------------------------ whole solves
+TISSUE = ["cube6_ms_f32", "cfg1_ms_f32", "cube8_ttp_f32", "ico3_crn_f32", "cube4_ms_period_f32", "cube4_ms_rt_f32"]
+
+
+@pytest.mark.parametrize("name", TISSUE)
+def test_monodomain_matches_reference(lib, cuda, name, tmp_path):
+    case = C.case(name)
+    g = golden(name)
+    out = tmp_path / "out"
+    sim, total = run_device_tissue(case, case_mesh_dir(case, tmp_path), cuda, result_dir=out)
+    AT = torch.load(out / "ATs.pt").numpy()
+    RT = torch.load(out / "RTs.pt").numpy()
+    Vm = torch.load(out / "Vm.pt").numpy()
+    assert Vm.shape[0] == int(case["T"] / 1.0) + 1 and Vm.shape[1] == len(AT)
+    if "Vm_idx" in g:
+        Vm = Vm[g["Vm_idx"]]
+    dt = case["dt"]
+    assert np.abs(AT - g["AT"]).max() <= dt * 1.001, np.abs(AT - g["AT"]).max()
+    assert np.abs(RT - g["RT"]).max() <= dt * 1.001, np.abs(RT - g["RT"]).max()
+    assert ((AT == -1) == (g["AT"] == -1)).all()
+    err = np.abs(Vm - g["Vm"]).max() / np.abs(g["Vm"]).max()
+    assert err <= 1e-3, err
+    ref_total = int(g["n_total_iter"])
+    assert abs(total - ref_total) <= max(3, ref_total // 50), (total, ref_total)
+
+
+@pytest.mark.parametrize("name,ref64", [("cfg1_ms_f32", "cfg1_ms_f64"), ("cube8_ttp_f32", "cube8_ttp_f64"),
+                                        ("ico3_crn_f32", "ico3_crn_f64")])
+def test_error_against_float64_reference(lib, cuda, name, ref64, tmp_path):
+    """FP32 bulk with FP64 CG reductions against a full-FP64 reference run."""
+    case = C.case(name)
+    g = golden(ref64)
+    out = tmp_path / "out"
+    run_device_tissue(case, case_mesh_dir(case, tmp_path), cuda, result_dir=out)
+    AT = torch.load(out / "ATs.pt").numpy()
+    Vm = torch.load(out / "Vm.pt").numpy()
+    if "Vm_idx" in g:
+        Vm = Vm[g["Vm_idx"]]
+    assert np.abs(AT - g["AT"]).max() <= case["dt"] * 1.001
+    assert np.abs(Vm - g["Vm"]).max() / np.abs(g["Vm"]).max() <= 1e-3
+
+
+def test_step_api_matches_oracle(lib, cuda, tmp_path):
+    """Monodomain.step with an explicit (u, t), as monodomain.py:109-139."""
+    case = C.case("cube6_ms_f32")
+    d = case_mesh_dir(case, tmp_path)
+    from torchcor_b200.simulator import Monodomain
+    sim = Monodomain(device_ionic(case, cuda), T=case["T"], dt=case["dt"], device=cuda)
+    sim.load_mesh(d)
+    for c in case["conductivity"]:
+        sim.add_conductivity(**c)
+    for s in case["stimuli"]:
+        sim.add_stimulus(str(d / s["file"]), s["start"], s["duration"], s["intensity"])
+    osim, _ = run_oracle_tissue(case, d, n_steps=5)
+    g = golden("cube6_ms_f32")
+    sim.assemble()
+    u = None
+    t = 0.0
+    iters = []
+    for n in range(5):
+        t += case["dt"]
+        if u is None:
+            sim._setup(case["tol"], case["tol"], case["max_iter"], True, True, 1, False)
+            u = sim.current_solution().clone()
+        u, it, _, _ = sim.step(u, t, case["tol"], case["tol"], case["max_iter"])
+        iters.append(it)
+        ref = g["traj"][n]
+        assert np.abs(u.cpu().numpy() - ref).max() <= 1e-4 * np.abs(ref).max()
+    assert iters == list(g["iters"][:5])
+
+
+def test_state_attributes_are_views(lib, cuda):
+    from torchcor_b200.ionic import TenTusscherPanfilov
+    m = TenTusscherPanfilov("ENDO", 0.01, device=cuda)
+    V = m.initialize(100)
+    assert V.shape == (100,) and float(V[0]) == pytest.approx(-86.2)
+    assert m.Cai.shape == (100,) and float(m.Cai[3]) == pytest.approx(0.00007)
+    m.Cai = torch.full((100,), 1e-4)
+    assert float(m.Cai[7]) == pytest.approx(1e-4)

@@ -1,0 +1,65 @@
+"""The oracle against the reference's own outputs (golden fixtures made by
+running TorchCor itself, tests/golden/make_golden.py).  CPU only.
+
+On the machine the fixtures were generated on, the restatement is bit-exact;
+elsewhere the CPU vector width changes the last bits of a few PyTorch ops
+(arange, transcendental functions), so values are compared with a tight
+tolerance and integer outputs (pattern, iteration counts) exactly.
+"""
+import numpy as np
+import pytest
+import torch
+
+from tests.golden import cases as C
+from tests.helpers import case_mesh_dir, golden, oracle_ionic, run_oracle_tissue
+
+TISSUE = ["cube6_ms_f32", "cube8_ttp_f32", "cube8_ttp_f64", "ico3_crn_f32", "ico3_crn_f64",
+          "cube4_ms_period_f32", "cfg1_ms_f32"]
+
+
+@pytest.mark.parametrize("name", TISSUE)
+def test_oracle_tissue(name, tmp_path):
+    torch.set_num_threads(8)
+    case = C.case(name)
+    g = golden(name)
+    sim, r = run_oracle_tissue(case, case_mesh_dir(case, tmp_path))
+    assert np.array_equal(r.system.A.crow_indices().numpy(), g["crow"])
+    assert np.array_equal(r.system.A.col_indices().numpy(), g["col"])
+    if "M" in g:
+        np.testing.assert_allclose(r.system.M.values().numpy(), g["M"], rtol=1e-6, atol=0)
+        np.testing.assert_allclose(r.system.K.values().numpy(), g["K"], rtol=1e-6, atol=1e-12)
+        np.testing.assert_allclose(r.system.PC.numpy(), g["PC"], rtol=1e-6)
+    assert abs(r.n_total_iter - int(g["n_total_iter"])) <= max(2, int(g["n_total_iter"]) // 200)
+    Vm = r.Vm.numpy()
+    if "Vm_idx" in g:
+        Vm = Vm[g["Vm_idx"]]
+    assert np.abs(Vm - g["Vm"]).max() <= 1e-3 * np.abs(g["Vm"]).max()
+    dt = case["dt"]
+    np.testing.assert_allclose(r.AT.numpy(), g["AT"], atol=dt * 1.001)
+    np.testing.assert_allclose(r.RT.numpy(), g["RT"], atol=dt * 1.001)
+
+
+@pytest.mark.parametrize("name", ["step_ms_f32", "step_ttp_f32", "step_ttp_epi_f32", "step_crn_f32",
+                                  "step_ttp_f64", "step_crn_f64"])
+def test_oracle_single_step(name):
+    case = C.case(name)
+    g = golden(name)
+    im = oracle_ionic(case)
+    V0, st0 = C.random_ionic_inputs(case)
+    im.initialize(len(V0))
+    if case["model"] == "ms":
+        im.H = torch.from_numpy(st0["H"])
+    else:
+        for k, v in st0.items():
+            im.s[k] = torch.from_numpy(v)
+    dV = im.differentiate(torch.from_numpy(V0)).numpy()
+    np.testing.assert_allclose(dV, g["dV"], rtol=1e-5, atol=1e-5)
+    states = {"H": im.H} if case["model"] == "ms" else im.s
+    for k, v in states.items():
+        np.testing.assert_allclose(v.numpy(), g["out_" + k], rtol=1e-5, atol=1e-6)
+
+
+def test_oracle_golden_pins_exist():
+    # every case declared has a fixture
+    for c in C.CASES:
+        assert (golden(c["name"]) is not None)

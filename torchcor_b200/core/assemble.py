@@ -1,0 +1,185 @@
+"""P1 assembly on the device (the role of ``torchcor/core/assemble.py``).
+
+``assemble_system`` builds, for one mesh, the CSR pattern and scatter map (host
+C++), the element matrices (one thread per element), the deterministic
+slot-ordered sums into CSR values, the monodomain system values and the
+sliced-ELL copy the solver streams.  ``Matrices3D`` / ``Matrices3DSurface``
+keep the reference's class names and return (K, M) as sparse CSR tensors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from torchcor_b200 import _lib
+from torchcor_b200._lib import check, ptr, stream_ptr
+
+PAD = 128
+
+
+def n_padded(n):
+    return (n + PAD - 1) // PAD * PAD
+
+
+@dataclass
+class Pattern:
+    n_nodes: int
+    k: int
+    rowptr: np.ndarray
+    col: np.ndarray
+    slot_ptr: np.ndarray
+    slot_src: np.ndarray
+    diag: np.ndarray
+
+    @property
+    def nnz(self):
+        return int(self.rowptr[-1])
+
+
+def build_pattern(elems: np.ndarray, n_nodes: int) -> Pattern:
+    """CSR pattern (equal to the reference's coalesce -> to_sparse_csr) and the
+    contribution map in the reference's COO order (host C++)."""
+    lib = _lib.load()
+    el = np.ascontiguousarray(elems, dtype=np.int32)
+    E, k = el.shape
+    nnz = C.c_int64()
+    check(lib.tcb_pattern_size(ptr(el), E, k, n_nodes, C.byref(nnz)))
+    rowptr = np.empty(n_nodes + 1, dtype=np.int32)
+    col = np.empty(nnz.value, dtype=np.int32)
+    slot_ptr = np.empty(nnz.value + 1, dtype=np.int32)
+    slot_src = np.empty(k * k * E, dtype=np.int32)
+    diag = np.empty(n_nodes, dtype=np.int32)
+    check(lib.tcb_pattern_build(ptr(el), E, k, n_nodes, ptr(rowptr), ptr(col), ptr(slot_ptr), ptr(slot_src),
+                                ptr(diag)))
+    return Pattern(n_nodes, k, rowptr, col, slot_ptr, slot_src, diag)
+
+
+def local_matrices(nodes, elems, sl, st, fibres):
+    """(ke (E,k,k), mw (E,)) on the device; mw = volume/20 or area/12."""
+    lib = _lib.load()
+    E, k = elems.shape
+    ke = torch.empty((E, k, k), device=nodes.device, dtype=torch.float32)
+    mw = torch.empty((E,), device=nodes.device, dtype=torch.float32)
+    check(lib.tcb_assemble_local(k, ptr(nodes), ptr(elems), E, ptr(sl), ptr(st), ptr(fibres), ptr(ke), ptr(mw),
+                                 stream_ptr()))
+    return ke, mw
+
+
+@dataclass
+class System:
+    """Device matrices of one monodomain system."""
+    n: int
+    n_pad: int
+    nnz: int
+    rowptr: torch.Tensor          # CSR pattern (int32)
+    col: torch.Tensor
+    m_val: torch.Tensor           # M
+    k_val: torch.Tensor           # K / chi
+    a_val: torch.Tensor           # Cm*M + theta*dt*K/chi
+    krhs_val: torch.Tensor        # ((1-theta)*dt) * K/chi
+    d_inv: torch.Tensor           # 1/diag(A), padded to n_pad
+    n_slices: int
+    slice_ptr: torch.Tensor       # sliced ELL (int64 offsets)
+    sell_col: torch.Tensor
+    sell_m: torch.Tensor
+    sell_k: torch.Tensor
+    sell_a: torch.Tensor
+
+    def csr(self, values):
+        return torch.sparse_csr_tensor(self.rowptr, self.col, values, size=(self.n, self.n))
+
+
+def assemble_system(nodes, elems_np, sl, st, fibres, dt, chi=140, cm=0.01, theta=0.5, pattern=None) -> System:
+    """Assemble M, K/chi, A and the Jacobi preconditioner (monodomain.py:83-106)."""
+    lib = _lib.load()
+    dev = nodes.device
+    n = nodes.shape[0]
+    n_pad = n_padded(n)
+    pat = pattern if pattern is not None else build_pattern(elems_np, n)
+    nnz = pat.nnz
+    k = pat.k
+    elems = torch.from_numpy(np.ascontiguousarray(elems_np, dtype=np.int32)).to(dev)
+    ke, mw = local_matrices(nodes, elems, sl, st, fibres)
+    slot_ptr = torch.from_numpy(pat.slot_ptr).to(dev)
+    slot_src = torch.from_numpy(pat.slot_src).to(dev)
+    k_val = torch.empty(nnz, device=dev, dtype=torch.float32)
+    m_val = torch.empty(nnz, device=dev, dtype=torch.float32)
+    s = stream_ptr()
+    check(lib.tcb_assemble_gather(k, ptr(slot_ptr), ptr(slot_src), nnz, ptr(ke), ptr(mw), ptr(k_val), ptr(m_val), s))
+    del ke, mw, slot_ptr, slot_src
+    diag = torch.from_numpy(pat.diag).to(dev)
+    a_val = torch.empty(nnz, device=dev, dtype=torch.float32)
+    krhs = torch.empty(nnz, device=dev, dtype=torch.float32)
+    d_inv = torch.empty(n_pad, device=dev, dtype=torch.float32)
+    check(lib.tcb_assemble_system(nnz, n, n_pad, ptr(diag), ptr(k_val), ptr(m_val), float(chi), float(cm), float(dt),
+                                  float(theta), ptr(a_val), ptr(krhs), ptr(d_inv), s))
+    # sliced ELL
+    n_slices = (n + _lib.TCB_SLICE - 1) // _lib.TCB_SLICE
+    sp = np.empty(n_slices + 1, dtype=np.int64)
+    n_entries = C.c_int64()
+    check(lib.tcb_sell_layout(ptr(pat.rowptr), n, ptr(sp), C.byref(n_entries)))
+    rowptr = torch.from_numpy(pat.rowptr).to(dev)
+    col = torch.from_numpy(pat.col).to(dev)
+    slice_ptr = torch.from_numpy(sp).to(dev)
+    ne = n_entries.value
+    sell_col = torch.empty(ne, device=dev, dtype=torch.int32)
+    sell = [torch.empty(ne, device=dev, dtype=torch.float32) for _ in range(3)]
+    vin = (C.c_void_p * 3)(ptr(m_val), ptr(krhs), ptr(a_val))
+    vout = (C.c_void_p * 3)(*[ptr(t) for t in sell])
+    check(lib.tcb_sell_pack(n, ptr(rowptr), ptr(col), ptr(slice_ptr), n_slices, 3, vin, ptr(sell_col), vout, s))
+    return System(n=n, n_pad=n_pad, nnz=nnz, rowptr=rowptr, col=col, m_val=m_val, k_val=k_val, a_val=a_val,
+                  krhs_val=krhs, d_inv=d_inv, n_slices=n_slices, slice_ptr=slice_ptr, sell_col=sell_col,
+                  sell_m=sell[0], sell_k=sell[1], sell_a=sell[2])
+
+
+class _Matrices:
+    k = 4
+
+    def __init__(self, vertices, elems, device, dtype):
+        self.vertices = vertices
+        self.elems = elems
+        self.device = device
+        self.dtype = dtype
+
+    def assemble_matrices(self, sigma_l, sigma_t, fibres):
+        """(K, M) as sparse CSR tensors.  The reference takes the (E,3,3) tensor;
+        here the per-element (sigma_l, sigma_t, fibre) it is formed from."""
+        el = self.elems.cpu().numpy() if isinstance(self.elems, torch.Tensor) else np.asarray(self.elems)
+        n = self.vertices.shape[0]
+        pat = build_pattern(el, n)
+        nodes = self.vertices.to(self.device, torch.float32).contiguous()
+        elems = torch.from_numpy(np.ascontiguousarray(el, dtype=np.int32)).to(self.device)
+        ke, mw = local_matrices(nodes, elems, sigma_l.to(self.device, torch.float32).contiguous(),
+                                sigma_t.to(self.device, torch.float32).contiguous(),
+                                fibres.to(self.device, torch.float32).contiguous())
+        lib = _lib.load()
+        dev = self.device
+        k_val = torch.empty(pat.nnz, device=dev, dtype=torch.float32)
+        m_val = torch.empty(pat.nnz, device=dev, dtype=torch.float32)
+        sp = torch.from_numpy(pat.slot_ptr).to(dev)
+        ss = torch.from_numpy(pat.slot_src).to(dev)
+        check(lib.tcb_assemble_gather(el.shape[1], ptr(sp), ptr(ss), pat.nnz, ptr(ke), ptr(mw), ptr(k_val),
+                                      ptr(m_val), stream_ptr()))
+        rp = torch.from_numpy(pat.rowptr).to(dev)
+        cl = torch.from_numpy(pat.col).to(dev)
+        K = torch.sparse_csr_tensor(rp, cl, k_val, size=(n, n))
+        M = torch.sparse_csr_tensor(rp, cl, m_val, size=(n, n))
+        return K, M
+
+
+class Matrices3D(_Matrices):
+    """P1 tetrahedra (assemble.py:148-248)."""
+
+    def __init__(self, vertices, tetrahedrons, device, dtype):
+        super().__init__(vertices, tetrahedrons, device, dtype)
+
+
+class Matrices3DSurface(_Matrices):
+    """P1 triangles of a surface embedded in 3-D (assemble.py:99-145)."""
+    k = 3
+
+    def __init__(self, vertices, triangles, device, dtype):
+        super().__init__(vertices, triangles, device, dtype)

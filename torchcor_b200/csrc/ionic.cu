@@ -1,0 +1,320 @@
+// Ionic-model kernels: lookup-table construction, initial state,
+// stand-alone differentiate(), and the fused per-step kernel of the
+// monodomain loop (activation/repolarisation update of the previous step,
+// snapshot, ionic update, stimulus injection and the right-hand side
+// b' = u*Cm + dt*du/100 + dt*Istim/100 of monodomain.py:117-128).
+//
+// Compiled with -fmad=false: every float32 operation rounds separately, as
+// the reference's element-wise tensor ops do.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include "ionic_crn.cuh"
+#include "ionic_ms.cuh"
+#include "ionic_ttp.cuh"
+#include "mono.cuh"
+#include "tcb_internal.h"
+
+namespace tcb {
+
+int64_t LutSpec::rows() const { return (int64_t)ceil((mx - mn) / res); }
+int32_t LutSpec::mx_idx() const { return (int32_t)((mx - mn) * (1.0 / res)) - 1; }
+Lut LutSpec::make(const float* tab) const {
+    Lut L;
+    L.tab = tab;
+    L.mn = (float)mn;
+    L.mx = (float)mx;
+    L.res = (float)res;
+    L.step = (float)(1.0 / res);
+    L.mx_idx = mx_idx();
+    return L;
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned grid_for(int64_t n) {
+    int64_t b = ceil_div(n, kThreads);
+    return (unsigned)(b > 148 * 64 ? 148 * 64 : b);
+}
+
+// ------------------------------------------------------------- tables
+// grid value of row i: float32(mn + i*res), computed in double
+__device__ inline float grid_value(double mn, double res, int64_t i) { return (float)(mn + (double)i * res); }
+
+__global__ void ttp_v_table(TTP::C c, float* tab, int64_t rows, double mn, double res) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
+        float o[TV_NCOL];
+        TTP::v_row(grid_value(mn, res, i), c, o);
+        for (int k = 0; k < TV_NCOL; ++k) tab[i * TV_NCOL + k] = o[k];
+    }
+}
+__global__ void ttp_cass_table(TTP::C c, float* tab, int64_t rows, double mn, double res) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
+        float o[3];
+        TTP::cass_row(grid_value(mn, res, i), c, o);
+        for (int k = 0; k < 3; ++k) tab[i * 3 + k] = o[k];
+    }
+}
+__global__ void ttp_vek_table(float* tab, int64_t rows, double mn, double res) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x)
+        tab[i] = TTP::vek_row(grid_value(mn, res, i));
+}
+__global__ void crn_v_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
+        float o[CV_NCOL];
+        CRN::v_row(grid_value(mn, res, i), c, o);
+        for (int k = 0; k < CV_NCOL; ++k) tab[i * CV_NCOL + k] = o[k];
+    }
+}
+__global__ void crn_cai_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
+        float o[CC_NCOL];
+        CRN::cai_row(grid_value(mn, res, i), c, o);
+        for (int k = 0; k < CC_NCOL; ++k) tab[i * CC_NCOL + k] = o[k];
+    }
+}
+__global__ void crn_fn_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
+        float o[3];
+        CRN::fn_row(grid_value(mn, res, i), c, o);
+        for (int k = 0; k < 3; ++k) tab[i * 3 + k] = o[k];
+    }
+}
+
+// ------------------------------------------------------------- init / differentiate
+template <class M>
+__global__ void init_kernel(typename M::C c, float* state, int64_t n_pad, float* v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += (int64_t)gridDim.x * blockDim.x) {
+        float s[M::kStates];
+        float V;
+        M::init(c, s, V);
+        for (int k = 0; k < M::kStates; ++k) state[k * n_pad + i] = s[k];
+        if (v) v[i] = V;
+    }
+}
+
+template <class M>
+__global__ void differentiate_kernel(typename M::C c, typename M::Tables T, float* state, int64_t n_pad, int64_t n,
+                                     const float* __restrict__ v, float* __restrict__ dv) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float s[M::kStates];
+#pragma unroll
+        for (int k = 0; k < M::kStates; ++k) s[k] = state[k * n_pad + i];
+        float d = M::step(v[i], s, c, T);
+#pragma unroll
+        for (int k = 0; k < M::kStates; ++k) state[k * n_pad + i] = s[k];
+        dv[i] = d;
+    }
+}
+
+// ------------------------------------------------------------- fused step kernel
+// activation / repolarisation update of monodomain.py:174-176 for time t
+__device__ __forceinline__ void at_rt_update(float u, float t, float* at, float* rt, int64_t i) {
+    float a = at[i];
+    if (u > 0.0f && a == -1.0f) {
+        a = t;
+        at[i] = a;
+    }
+    if (a > 0.0f && u < -70.0f && rt[i] == -1.0f) rt[i] = t;
+}
+
+template <class M>
+__global__ void __launch_bounds__(kThreads) mono_ionic_kernel(MonoDev d, typename M::C c, typename M::Tables T) {
+    const int64_t n = d.counter[0];  // this step (1-based)
+    const float* __restrict__ u = d.x + ring_cur(n) * d.n_pad;
+    const int64_t prev = n - 1;
+    const bool do_atrt = d.at_rt && prev >= 1;
+    const float t_prev = d.step_t[prev];
+    float* snap = (d.snap && d.per_frame > 0 && prev >= 1 && prev % d.per_frame == 0)
+                      ? d.snap + (prev / d.per_frame) * d.n
+                      : nullptr;
+    const uint32_t smask = d.step_stim[n];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = u[i];
+        if (do_atrt) at_rt_update(v, t_prev, d.at, d.rt, i);
+        if (snap) snap[i] = v;
+        float s[M::kStates];
+#pragma unroll
+        for (int k = 0; k < M::kStates; ++k) s[k] = d.state[k * d.n_pad + i];
+        const float dV = M::step(v, s, c, T);
+#pragma unroll
+        for (int k = 0; k < M::kStates; ++k) d.state[k * d.n_pad + i] = s[k];
+        // b = u*Cm + dt*du, du = dV/100  (monodomain.py:117-118)
+        float b = v * d.cm + d.dt * (dV / 100.0f);
+        if (smask) {
+            // Istim = sum of the active stimuli in list order (stimulation.py:59-61), /100 (:127)
+            uint32_t bits = d.stim_bits[i] & smask;
+            if (bits) {
+                float I = 0.0f;
+                bool first = true;
+                for (int k = 0; k < TCB_MAX_STIMULI; ++k) {
+                    if ((smask >> k) & 1u) {
+                        float a = ((bits >> k) & 1u) ? d.amp[k] : 0.0f;
+                        I = first ? a : I + a;
+                        first = false;
+                    }
+                }
+                b = b + d.dt * (I / 100.0f);
+            }
+        }
+        d.bp[i] = b;
+    }
+}
+
+__global__ void mono_finish_kernel(MonoDev d) {
+    const int64_t n = d.counter[0];  // nt + 1 after the last step
+    const int64_t last = n - 1;
+    if (last < 1) return;
+    const float* u = d.x + ring_cur(n) * d.n_pad;
+    const float t = d.step_t[last];
+    float* snap = (d.snap && d.per_frame > 0 && last % d.per_frame == 0) ? d.snap + (last / d.per_frame) * d.n : nullptr;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += (int64_t)gridDim.x * blockDim.x) {
+        float v = u[i];
+        if (d.at_rt) at_rt_update(v, t, d.at, d.rt, i);
+        if (snap) snap[i] = v;
+    }
+}
+
+template <class M>
+int launch_mono(const tcb_mono* m, const MonoDev& d, cudaStream_t s) {
+    typename M::C c = M::derive(m->params);
+    typename M::Tables T = M::tables(m->tables, m->params);
+    mono_ionic_kernel<M><<<grid_for(d.n), kThreads, 0, s>>>(d, c, T);
+    TCB_CHECK_LAUNCH("mono ionic kernel");
+    return TCB_OK;
+}
+
+template <class M>
+int run_init(const double* params, float* state, int64_t n_pad, float* v, cudaStream_t s) {
+    init_kernel<M><<<grid_for(n_pad), kThreads, 0, s>>>(M::derive(params), state, n_pad, v);
+    TCB_CHECK_LAUNCH("init kernel");
+    return TCB_OK;
+}
+
+template <class M>
+int run_differentiate(const double* params, const float* tables, float* state, int64_t n_pad, int64_t n,
+                      const float* v, float* dv, cudaStream_t s) {
+    differentiate_kernel<M><<<grid_for(n), kThreads, 0, s>>>(M::derive(params), M::tables(tables, params), state,
+                                                             n_pad, n, v, dv);
+    TCB_CHECK_LAUNCH("differentiate kernel");
+    return TCB_OK;
+}
+
+}  // namespace
+
+int launch_mono_ionic(const tcb_mono* m, const MonoDev& d, cudaStream_t s) {
+    switch (m->model) {
+        case TCB_MODEL_MS: return launch_mono<MS>(m, d, s);
+        case TCB_MODEL_TTP: return launch_mono<TTP>(m, d, s);
+        case TCB_MODEL_CRN: return launch_mono<CRN>(m, d, s);
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+int launch_mono_finish(const MonoDev& d, cudaStream_t s) {
+    mono_finish_kernel<<<grid_for(d.n), kThreads, 0, s>>>(d);
+    TCB_CHECK_LAUNCH("mono finish kernel");
+    return TCB_OK;
+}
+
+}  // namespace tcb
+
+using namespace tcb;
+
+extern "C" const char* tcb_model_params(int32_t model) {
+    switch (model) {
+        case TCB_MODEL_MS: return TCB_MS_PARAMS;
+        case TCB_MODEL_TTP: return TCB_TTP_PARAMS;
+        case TCB_MODEL_CRN: return TCB_CRN_PARAMS;
+    }
+    return nullptr;
+}
+
+extern "C" const char* tcb_model_states(int32_t model) {
+    switch (model) {
+        case TCB_MODEL_MS: return TCB_MS_STATES;
+        case TCB_MODEL_TTP: return TCB_TTP_STATES;
+        case TCB_MODEL_CRN: return TCB_CRN_STATES;
+    }
+    return nullptr;
+}
+
+extern "C" int tcb_model_layout(int32_t model, const double* params, int64_t* n_states, int64_t* table_floats) {
+    if (!n_states || !table_floats) return fail(TCB_EINVAL, "tcb_model_layout: null output");
+    switch (model) {
+        case TCB_MODEL_MS:
+            *n_states = MS::kStates;
+            *table_floats = MS::table_floats(params);
+            return TCB_OK;
+        case TCB_MODEL_TTP:
+            *n_states = TTP::kStates;
+            *table_floats = TTP::table_floats(params);
+            return TCB_OK;
+        case TCB_MODEL_CRN:
+            *n_states = CRN::kStates;
+            *table_floats = CRN::table_floats(params);
+            return TCB_OK;
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+extern "C" int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream) {
+    if (!params) return fail(TCB_EINVAL, "tcb_model_tables: null params");
+    cudaStream_t s = as_stream(stream);
+    if (model == TCB_MODEL_MS) return TCB_OK;
+    if (!tables) return fail(TCB_EINVAL, "tcb_model_tables: null tables");
+    if (model == TCB_MODEL_TTP) {
+        TTP::C c = TTP::derive(params);
+        TTP::Tables T = TTP::tables(tables, params);
+        ttp_v_table<<<grid_for(TTP::kV.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.V.tab), TTP::kV.rows(),
+                                                                    TTP::kV.mn, TTP::kV.res);
+        ttp_cass_table<<<grid_for(TTP::kCaSS.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.CaSS.tab),
+                                                                          TTP::kCaSS.rows(), TTP::kCaSS.mn,
+                                                                          TTP::kCaSS.res);
+        ttp_vek_table<<<grid_for(TTP::kVEk.rows()), kThreads, 0, s>>>(const_cast<float*>(T.VEk.tab),
+                                                                        TTP::kVEk.rows(), TTP::kVEk.mn, TTP::kVEk.res);
+        TCB_CHECK_LAUNCH("TTP table kernels");
+        return TCB_OK;
+    }
+    if (model == TCB_MODEL_CRN) {
+        CRN::C c = CRN::derive(params);
+        CRN::Tables T = CRN::tables(tables, params);
+        crn_v_table<<<grid_for(CRN::kV.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.V.tab), CRN::kV.rows(),
+                                                                    CRN::kV.mn, CRN::kV.res);
+        crn_cai_table<<<grid_for(CRN::kCai.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.Cai.tab),
+                                                                        CRN::kCai.rows(), CRN::kCai.mn, CRN::kCai.res);
+        crn_fn_table<<<grid_for(CRN::kFn.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.Fn.tab), CRN::kFn.rows(),
+                                                                      CRN::kFn.mn, CRN::kFn.res);
+        TCB_CHECK_LAUNCH("CRN table kernels");
+        return TCB_OK;
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+extern "C" int tcb_model_init(int32_t model, const double* params, float* state, int64_t n_pad, float* v,
+                              void* stream) {
+    if (!params || !state || n_pad <= 0) return fail(TCB_EINVAL, "tcb_model_init: bad arguments");
+    cudaStream_t s = as_stream(stream);
+    switch (model) {
+        case TCB_MODEL_MS: return run_init<MS>(params, state, n_pad, v, s);
+        case TCB_MODEL_TTP: return run_init<TTP>(params, state, n_pad, v, s);
+        case TCB_MODEL_CRN: return run_init<CRN>(params, state, n_pad, v, s);
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+extern "C" int tcb_model_differentiate(int32_t model, const double* params, const float* tables, float* state,
+                                       int64_t n_pad, int64_t n, const float* v, float* dv, void* stream) {
+    if (!params || !state || !v || !dv || n <= 0 || n_pad < n) return fail(TCB_EINVAL, "tcb_model_differentiate: bad arguments");
+    if (model != TCB_MODEL_MS && !tables) return fail(TCB_EINVAL, "tcb_model_differentiate: null tables");
+    cudaStream_t s = as_stream(stream);
+    switch (model) {
+        case TCB_MODEL_MS: return run_differentiate<MS>(params, tables, state, n_pad, n, v, dv, s);
+        case TCB_MODEL_TTP: return run_differentiate<TTP>(params, tables, state, n_pad, n, v, dv, s);
+        case TCB_MODEL_CRN: return run_differentiate<CRN>(params, tables, state, n_pad, n, v, dv, s);
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}

@@ -1,0 +1,77 @@
+// Arithmetic helpers shared by the ionic-model kernels.
+//
+// The kernels reproduce the float32 operation order of the reference's
+// PyTorch expressions (the ionic translation units are compiled with
+// -fmad=false so a*b+c stays two roundings, as in separate tensor ops):
+//  * a Python float meeting a float32 tensor is rounded to float32 first;
+//  * `python_float / tensor` is evaluated by PyTorch as
+//    `tensor.reciprocal() * python_float` -> sdiv() below;
+//  * `tensor / python_float` is a true division by the rounded float.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace tcb {
+
+// number of comma-separated names in a parameter list (compile-time check
+// that a model's raw-parameter struct matches the names the host passes)
+constexpr int count_names(const char* s) {
+    int n = 1;
+    for (; *s; ++s) n += (*s == ',');
+    return n;
+}
+
+// python_float / tensor
+__device__ __forceinline__ float sdiv(float s, float t) { return (1.0f / t) * s; }
+
+// torch.clamp(X, mn, mx) with NaN propagation
+__device__ __forceinline__ float tclamp(float x, float mn, float mx) {
+    x = (x < mn) ? mn : x;
+    return (x > mx) ? mx : x;
+}
+
+// Lookup table with the reference's linear interpolation
+// (TenTusscherPanfilov.py:188-195, CourtemancheRamirezNattel.py:203-210).
+struct Lut {
+    const float* tab;   // rows x ncol, row-major
+    float mn, mx, res, step;
+    int32_t mx_idx;
+};
+
+struct LutPos {
+    int32_t lo;
+    float w, w1;  // w, 1 - w
+};
+
+__device__ __forceinline__ LutPos lut_pos(float X, const Lut& L) {
+    X = tclamp(X, L.mn, L.mx);
+    float f = (X - L.mn) * L.step;
+    long long idx = (f != f) ? 0 : (long long)f;   // .to(torch.long) truncates
+    idx = idx < 0 ? 0 : idx;
+    idx = idx > (long long)(L.mx_idx - 1) ? (long long)(L.mx_idx - 1) : idx;
+    float lo_pos = (float)idx * L.res + L.mn;
+    float w = (X - lo_pos) / L.res;
+    LutPos p;
+    p.lo = (int32_t)idx;
+    p.w = w;
+    p.w1 = 1.0f - w;
+    return p;
+}
+
+template <int NCOL>
+__device__ __forceinline__ float lut_col(const Lut& L, const LutPos& p, int c) {
+    const float* r0 = L.tab + (int64_t)p.lo * NCOL;
+    return p.w1 * __ldg(r0 + c) + p.w * __ldg(r0 + NCOL + c);
+}
+
+// host-side helpers describing a table the way the reference does
+struct LutSpec {
+    double mn, mx, res;
+    int ncol;
+    int64_t rows() const;       // torch.arange(mn, mx, res).shape[0]
+    int32_t mx_idx() const;     // int((mx - mn) * (1/res)) - 1
+    Lut make(const float* tab) const;
+};
+
+}  // namespace tcb

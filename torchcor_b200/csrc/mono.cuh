@@ -1,0 +1,41 @@
+// Device view of one monodomain simulation (built from tcb_mono on the host).
+#pragma once
+#include <stdint.h>
+
+#include "tcb200.h"
+
+namespace tcb {
+
+struct MonoDev {
+    int64_t n, n_pad, n_slices, nt;
+    const int64_t* slice_ptr;
+    const int32_t* col;
+    const float *mv, *kv, *av, *dinv;
+    float* state;
+    float *x, *bp, *r, *p, *ap, *at, *rt, *snap;
+    const uint32_t* stim_bits;
+    const float* step_t;
+    const uint32_t* step_stim;
+    int32_t* step_iters;
+    int32_t* counter;
+    double* scratch;
+    uint32_t* bar;
+    double a_tol, r_tol;
+    int32_t max_iter, linear_guess, at_rt, per_frame;
+    float cm, dt;
+    float amp[TCB_MAX_STIMULI];
+};
+
+MonoDev make_dev(const tcb_mono* m);
+
+// membrane-potential ring: step n reads slot (n-1)%3, guesses from (n+1)%3, writes n%3
+__host__ __device__ inline int64_t ring_cur(int64_t n) { return (n + 2) % 3; }
+__host__ __device__ inline int64_t ring_prev(int64_t n) { return (n + 1) % 3; }
+__host__ __device__ inline int64_t ring_next(int64_t n) { return n % 3; }
+
+// launchers implemented in ionic.cu / cg.cu
+int launch_mono_ionic(const tcb_mono* m, const MonoDev& d, cudaStream_t s);
+int launch_mono_finish(const MonoDev& d, cudaStream_t s);
+int launch_cg(const MonoDev& d, cudaStream_t s);
+
+}  // namespace tcb

@@ -1,0 +1,4 @@
+"""Simulators (``torchcor.simulator`` names)."""
+from torchcor_b200.simulator.monodomain import Monodomain
+
+__all__ = ["Monodomain"]

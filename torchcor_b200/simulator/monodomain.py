@@ -1,0 +1,226 @@
+"""``Monodomain`` with the interface of ``torchcor/simulator/monodomain.py:18-226``.
+
+The time loop runs on the device: per step one ionic kernel (activation and
+repolarisation update of the previous step, snapshot, ionic model, stimulus,
+right-hand side) and one persistent cooperative kernel (mass/stiffness
+products, extrapolated guess, Jacobi-PCG with the stopping test on the
+device).  The host only launches; the step index, CG iteration counts and the
+membrane-potential ring live in device memory, so a solve needs no host
+synchronisation until it finishes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from torchcor_b200 import _lib
+from torchcor_b200._lib import check, ptr, stream_ptr
+from torchcor_b200.core.assemble import assemble_system
+from torchcor_b200.core.conductivity import Conductivity
+from torchcor_b200.core.mesh import MeshReader
+from torchcor_b200.core.stimulation import Stimuli
+from torchcor_b200.device import get_device
+
+
+class Monodomain:
+    def __init__(self, ionic_model, T, dt, device=None, dtype=None):
+        self.device = torch.device(device) if device is not None else get_device()
+        if self.device.type != "cuda":
+            raise RuntimeError("torchcor_b200.Monodomain needs a CUDA device (no CPU fallback)")
+        if dtype not in (None, torch.float32):
+            raise NotImplementedError("torchcor_b200 runs the monodomain step in float32 "
+                                      "(float64 inner products inside CG)")
+        self.dtype = torch.float32
+        self.T = T
+        self.dt = dt
+        self.nt = int(T / dt)                                  # monodomain.py:25
+        self.ionic_model = ionic_model
+        if getattr(ionic_model, "dt", None) is None:
+            ionic_model.dt = dt
+        self.Chi, self.Cm, self.theta = 140, 0.01, 0.5          # :44-46
+        self.n_nodes = None
+        self.nodes = self.elems = self.regions = self.fibres = None
+        self.stimuli = None
+        self.conductivity = None
+        self.system = None
+        self.K = self.M = self.A = None
+        self.mesh_path = None
+        self.result_path = None
+        self._sim = None
+
+    # ------------------------------------------------------------------ input
+    def load_mesh(self, path="Data/ventricle/Case_1", unit_conversion=1000):
+        self.mesh_path = Path(path)
+        nodes, elems, regions, fibres = MeshReader(path).read(unit_conversion=unit_conversion)
+        self.load_arrays(nodes, elems, regions, fibres)
+
+    def load_arrays(self, nodes, elems, regions, fibres):
+        """Mesh already in memory: nodes (N,3) in mm, elems (E,3|4), per-element regions and fibres."""
+        self.n_nodes = int(nodes.shape[0])
+        self._elems_np = np.ascontiguousarray(elems, dtype=np.int32)
+        self.nodes = torch.from_numpy(np.asarray(nodes)).to(dtype=torch.float32, device=self.device)
+        self.elems = torch.from_numpy(self._elems_np).to(device=self.device)
+        self.regions = torch.from_numpy(np.ascontiguousarray(regions)).to(dtype=torch.int, device=self.device)
+        self.fibres = torch.from_numpy(np.asarray(fibres)).to(dtype=torch.float32, device=self.device)
+        self.stimuli = Stimuli(self.n_nodes, self.device, self.dtype)
+        self.conductivity = Conductivity(self.regions, dtype=self.dtype)
+
+    def add_stimulus(self, vtx_filepath, start, duration, intensity, period=None, count=1, region=None):
+        if period is None:
+            period = self.T
+        self.stimuli.add(vtx_filepath, start, duration, intensity, period, count, region=region)
+
+    def add_conductivity(self, region_ids, il, it, el=None, et=None):
+        self.conductivity.add(region_ids, il, it, el, et)
+
+    # --------------------------------------------------------------- assembly
+    def assemble(self):
+        c = self.conductivity
+        self.system = assemble_system(self.nodes, self._elems_np, c.sigma_l.contiguous(), c.sigma_t.contiguous(),
+                                      self.fibres.contiguous(), self.dt, self.Chi, self.Cm, self.theta)
+        s = self.system
+        self.M = s.csr(s.m_val)
+        self.K = s.csr(s.k_val)
+        self.A = s.csr(s.a_val)
+        return s
+
+    # -------------------------------------------------------------- time loop
+    def _setup(self, a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep_snapshots):
+        s = self.system
+        dev = self.device
+        im = self.ionic_model
+        u0 = im.initialize(self.n_nodes)
+        n, n_pad, nt = s.n, s.n_pad, self.nt
+        f32 = dict(device=dev, dtype=torch.float32)
+        x = torch.zeros((3, n_pad), **f32)
+        x[0, :n] = u0
+        x[2, :n] = u0                                          # x_prev = x at initialise (solver.py:26)
+        per_frame = int(snapshot_interval / self.dt)           # :150
+        if per_frame == 0:
+            raise ZeroDivisionError("snapshot_interval is shorter than dt")
+        n_snap = nt // per_frame + 1
+        snaps = torch.empty((n_snap, n), **f32) if keep_snapshots else None
+        if snaps is not None:
+            snaps[0] = u0
+        t32, mask = self.stimuli.schedule(nt, self.dt)
+        sim = dict(
+            x=x, bp=torch.zeros(n_pad, **f32), r=torch.zeros(n_pad, **f32), p=torch.zeros(n_pad, **f32),
+            ap=torch.zeros(n_pad, **f32), at=torch.full((n,), -1.0, **f32), rt=torch.full((n,), -1.0, **f32),
+            snaps=snaps, u0=u0,
+            stim_bits=torch.from_numpy(self.stimuli.membership_bits().view(np.int32)).to(dev),
+            step_t=torch.from_numpy(t32).to(dev), step_stim=torch.from_numpy(mask.view(np.int32)).to(dev),
+            step_iters=torch.zeros(nt + 1, device=dev, dtype=torch.int32),
+            counter=torch.tensor([1, 0, 0, 0], device=dev, dtype=torch.int32),
+            scratch=torch.zeros(int(_lib.load().tcb_mono_scratch_doubles()), device=dev, dtype=torch.float64),
+            barrier=torch.zeros(4, device=dev, dtype=torch.int32),
+            params=im.param_array(), per_frame=per_frame, next_step=1,
+        )
+        m = _lib.tcb_mono()
+        m.n_nodes, m.n_pad, m.n_slices, m.nt = n, n_pad, s.n_slices, nt
+        m.model, m.n_states = im.model_id, im.state.shape[0]
+        m.slice_ptr, m.col = ptr(s.slice_ptr), ptr(s.sell_col)
+        m.m_val, m.k_val, m.a_val, m.d_inv = ptr(s.sell_m), ptr(s.sell_k), ptr(s.sell_a), ptr(s.d_inv)
+        m.state, m.tables = ptr(im.state), ptr(im.tables)
+        m.x, m.bprime, m.r, m.p, m.ap = (ptr(sim[k]) for k in ("x", "bp", "r", "p", "ap"))
+        m.at, m.rt, m.snapshots = ptr(sim["at"]), ptr(sim["rt"]), ptr(snaps)
+        m.stim_bits, m.step_t, m.step_stim = ptr(sim["stim_bits"]), ptr(sim["step_t"]), ptr(sim["step_stim"])
+        amp = self.stimuli.amplitudes()
+        for k in range(_lib.TCB_MAX_STIMULI):
+            m.stim_amp[k] = float(amp[k])
+        m.a_tol, m.r_tol, m.max_iter = float(a_tol), float(r_tol), int(max_iter)
+        m.linear_guess, m.at_rt, m.per_frame = int(bool(linear_guess)), int(bool(calculate_AT_RT)), per_frame
+        m.cm, m.dt = float(self.Cm), float(self.dt)
+        m.step_iters, m.counter = ptr(sim["step_iters"]), ptr(sim["counter"])
+        m.scratch, m.barrier = ptr(sim["scratch"]), ptr(sim["barrier"])
+        m.params = sim["params"].ctypes.data
+        sim["struct"] = m
+        self._sim = sim
+        return sim
+
+    def run_steps(self, n_steps, stream=None):
+        """Advance the prepared simulation by ``n_steps`` steps (asynchronous)."""
+        sim = self._sim
+        a = sim["next_step"]
+        b = min(a + n_steps, self.nt + 1)
+        if b > a:
+            check(_lib.load().tcb_mono_run(C.byref(sim["struct"]), a, b, stream_ptr(stream)))
+        sim["next_step"] = b
+        return b - a
+
+    def current_solution(self):
+        sim = self._sim
+        return sim["x"][(sim["next_step"] + 2) % 3, : self.n_nodes]
+
+    def step(self, u, t, a_tol, r_tol, max_iter, verbose=False):
+        """One step of the prepared simulation (monodomain.py:109-139).  ``u`` must be
+        the previous solution and ``t`` the time of this step; returns
+        (u, n_iter, ionic_time, electric_time)."""
+        if self._sim is None:
+            if self.system is None:
+                self.assemble()
+            self._setup(a_tol, r_tol, max_iter, True, True, 1, False)
+        sim = self._sim
+        n = sim["next_step"]
+        if n > self.nt:
+            raise RuntimeError("all time steps of this simulation have been run")
+        sim["x"][(n + 2) % 3, : self.n_nodes] = u
+        sim["step_t"][n] = float(t)
+        m = 0
+        for k, s in enumerate(self.stimuli.stimulus_list):
+            if self.stimuli.is_active(s, t):
+                m |= 1 << k
+        sim["step_stim"][n] = np.int32(np.uint32(m).view(np.int32))
+        st = sim["struct"]
+        st.a_tol, st.r_tol, st.max_iter = float(a_tol), float(r_tol), int(max_iter)
+        t0 = time.time()
+        self.run_steps(1)
+        check(_lib.load().tcb_mono_check(C.byref(st), stream_ptr()))
+        el = time.time() - t0
+        return self.current_solution().clone(), int(sim["step_iters"][n].item()), 0.0, el
+
+    def solve(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1,
+              verbose=True, result_path=None):
+        self.result_path = Path(result_path) if result_path is not None else None
+        if self.result_path is not None:
+            self.result_path.mkdir(parents=True, exist_ok=True)
+        self.assemble()
+        keep = snapshot_interval < self.T
+        sim = self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep)
+        t0 = time.time()
+        chunk = max(1, sim["per_frame"]) * (1 if verbose and snapshot_interval != self.T else 1000)
+        while sim["next_step"] <= self.nt:
+            self.run_steps(chunk)
+            if verbose and snapshot_interval != self.T:
+                torch.cuda.synchronize(self.device)
+                done = sim["next_step"] - 1
+                print(f"t: {round(done * self.dt, 1)}/{self.T}", "Time elapsed:", round(time.time() - t0, 2),
+                      flush=True)
+        st = sim["struct"]
+        lib = _lib.load()
+        check(lib.tcb_mono_finish(C.byref(st), stream_ptr()))
+        check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
+        elapsed = time.time() - t0
+        n_total_iter = int(sim["step_iters"].sum().item())
+        self.n_total_iter = n_total_iter
+        self.activation_time = sim["at"]
+        self.repolarization_time = sim["rt"]
+        self.solutions = sim["snaps"]
+        if self.result_path is not None:
+            if calculate_AT_RT:
+                torch.save(sim["at"].cpu(), self.result_path / "ATs.pt")
+                torch.save(sim["rt"].cpu(), self.result_path / "RTs.pt")
+            if keep:
+                torch.save(sim["snaps"].cpu(), self.result_path / "Vm.pt")
+        if verbose:
+            mem = torch.cuda.max_memory_allocated(self.device) / 1e9
+            print(self.ionic_model.name, self.n_nodes, round(elapsed, 2), 0.0, round(elapsed, 2), n_total_iter,
+                  "n/a", f"{round(mem, 2)}", flush=True)
+            if calculate_AT_RT:
+                at, rt = sim["at"].cpu(), sim["rt"].cpu()
+                print("ATs: ", at.min().item(), at.max().item(), flush=True)
+                print("RTs: ", rt.min().item(), rt.max().item(), flush=True)
+        return n_total_iter
