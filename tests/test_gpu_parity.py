@@ -22,6 +22,13 @@ def rel_err(a, b):
 
 
 # ------------------------------------------------------------------ tables
+# V rows next to removable singularities of the CRN formulas ((V-a)/(1-exp(..))
+# at a = -47.13, -14.1, 3.3328, 19.9, 7.9; tau_d at -10): there the reference's
+# own float32 value is dominated by the last ulp of exp, so any two exp
+# implementations disagree; those rows are checked for finiteness only.
+CRN_SINGULAR = (-47.13, -14.1, 3.3328, 19.9, 7.9, -10.0)
+
+
 @pytest.mark.parametrize("model,kw", [("ttp", dict(cell_type="ENDO", dt=0.01)), ("ttp", dict(cell_type="EPI", dt=0.02)),
                                       ("crn", dict(dt=0.02)), ("crn", dict(dt=0.01))])
 def test_lookup_tables(lib, cuda, model, kw):
@@ -32,16 +39,26 @@ def test_lookup_tables(lib, cuda, model, kw):
     dev.initialize(16)
     t = dev.tables.cpu().numpy()
     if model == "ttp":
-        parts = [ref.V_tab, ref.CaSS_tab, ref.VEk_tab]
+        parts = [(ref.V_tab, None), (ref.CaSS_tab, None), (ref.VEk_tab, None)]
     else:
-        parts = [ref.V_tab, ref.Cai_tab, ref.fn_tab]
+        grid = torch.arange(-200., 200., 0.1).numpy()
+        near = np.zeros(len(grid), dtype=bool)
+        for a in CRN_SINGULAR:
+            near |= np.abs(grid - a) < 0.15
+        parts = [(ref.V_tab, near), (ref.Cai_tab, None), (ref.fn_tab, None)]
     off = 0
-    for p in parts:
+    for p, skip in parts:
         p = p.numpy()
         got = t[off:off + p.size].reshape(p.shape)
         off += p.size
-        # grid points differ from torch.arange's vectorised float32 grid by <= 1 ulp
-        np.testing.assert_allclose(got, p, rtol=2e-4, atol=1e-6 * np.abs(p).max(axis=0) + 1e-30)
+        assert np.isfinite(got).all()
+        # same float32 grid as torch.arange; exp/log/expm1 differ by a few ulp
+        tol = 1e-5 * np.abs(p) + 1e-7 * np.abs(p).max(axis=0)
+        ok = np.abs(got - p) <= tol
+        if skip is not None:
+            ok[skip] = True
+        assert ok.all(), (np.nonzero(~ok)[0][:10], np.nonzero(~ok)[1][:10])
+        assert (got == p).mean() > 0.75
     assert off == t.size
 
 

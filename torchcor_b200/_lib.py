@@ -112,11 +112,15 @@ def check(status):
 
 
 def ptr(t):
-    """Device/host address of a tensor or numpy array (None -> NULL)."""
+    """Device/host address of a C-contiguous tensor or numpy array (None -> NULL)."""
     if t is None:
         return None
     if isinstance(t, np.ndarray):
+        if not t.flags["C_CONTIGUOUS"]:
+            raise ValueError("array passed to libtcb200 must be C-contiguous")
         return t.ctypes.data
+    if not t.is_contiguous():
+        raise ValueError("tensor passed to libtcb200 must be contiguous")
     return t.data_ptr()
 
 

@@ -17,7 +17,7 @@ import pandas as pd
 def _table(path, usecols=None, dtype=None):
     df = pd.read_csv(path, sep=r"\s+", header=None, skiprows=1, usecols=usecols, dtype=dtype,
                      float_precision="round_trip", engine="c")
-    return df.to_numpy()
+    return np.ascontiguousarray(df.to_numpy())
 
 
 class MeshReader:

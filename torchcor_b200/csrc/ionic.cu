@@ -41,45 +41,63 @@ inline unsigned grid_for(int64_t n) {
 }
 
 // ------------------------------------------------------------- tables
-// grid value of row i: float32(mn + i*res), computed in double
-__device__ inline float grid_value(double mn, double res, int64_t i) { return (float)(mn + (double)i * res); }
+// Grid value of row i of a table built on torch.arange(mn, mx, res) in
+// float32 on the CPU, as PyTorch's CPU kernel forms it: the range is split
+// into chunks of max(32768, ceil(rows/8)) (its parallel grain on the 8-thread
+// host the reference fixtures come from); inside a chunk, whole 16-element
+// groups are vectorised as 8-wide vectors whose first element is
+// float(fma(res, i0, mn)) and whose element k is float(fma(k, res, first));
+// the remaining elements take float(fma(res, i, mn)).  The exact grid matters
+// at removable singularities of the table formulas (e.g. V = 7.9 in CRN tau_w).
+__device__ inline float grid_value(double mn, double res, int64_t i, int64_t rows) {
+    const int64_t chunk = rows / 8 + (rows % 8 != 0) > 32768 ? rows / 8 + (rows % 8 != 0) : 32768;
+    const int64_t cb = (i / chunk) * chunk;
+    const int64_t ce = cb + chunk < rows ? cb + chunk : rows;
+    const int64_t vec_end = cb + ((ce - cb) / 16) * 16;
+    if (i < vec_end) {
+        const int64_t i0 = cb + ((i - cb) / 8) * 8;
+        const float base = (float)__fma_rn(res, (double)i0, mn);
+        return (float)__fma_rn((double)(i - i0), res, (double)base);
+    }
+    return (float)__fma_rn(res, (double)i, mn);
+}
 
 __global__ void ttp_v_table(TTP::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[TV_NCOL];
-        TTP::v_row(grid_value(mn, res, i), c, o);
+        TTP::v_row(grid_value(mn, res, i, rows), c, o);
         for (int k = 0; k < TV_NCOL; ++k) tab[i * TV_NCOL + k] = o[k];
     }
 }
 __global__ void ttp_cass_table(TTP::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[3];
-        TTP::cass_row(grid_value(mn, res, i), c, o);
+        TTP::cass_row(grid_value(mn, res, i, rows), c, o);
         for (int k = 0; k < 3; ++k) tab[i * 3 + k] = o[k];
     }
 }
 __global__ void ttp_vek_table(float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x)
-        tab[i] = TTP::vek_row(grid_value(mn, res, i));
+        tab[i] = TTP::vek_row(grid_value(mn, res, i, rows));
 }
 __global__ void crn_v_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[CV_NCOL];
-        CRN::v_row(grid_value(mn, res, i), c, o);
+        CRN::v_row(grid_value(mn, res, i, rows), c, o);
         for (int k = 0; k < CV_NCOL; ++k) tab[i * CV_NCOL + k] = o[k];
     }
 }
 __global__ void crn_cai_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[CC_NCOL];
-        CRN::cai_row(grid_value(mn, res, i), c, o);
+        CRN::cai_row(grid_value(mn, res, i, rows), c, o);
         for (int k = 0; k < CC_NCOL; ++k) tab[i * CC_NCOL + k] = o[k];
     }
 }
 __global__ void crn_fn_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[3];
-        CRN::fn_row(grid_value(mn, res, i), c, o);
+        CRN::fn_row(grid_value(mn, res, i, rows), c, o);
         for (int k = 0; k < 3; ++k) tab[i * 3 + k] = o[k];
     }
 }

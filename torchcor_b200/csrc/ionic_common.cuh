@@ -22,11 +22,13 @@ constexpr int count_names(const char* s) {
     return n;
 }
 
+#define TCB_HD __host__ __device__ __forceinline__
+
 // python_float / tensor
-__device__ __forceinline__ float sdiv(float s, float t) { return (1.0f / t) * s; }
+TCB_HD float sdiv(float s, float t) { return (1.0f / t) * s; }
 
 // torch.clamp(X, mn, mx) with NaN propagation
-__device__ __forceinline__ float tclamp(float x, float mn, float mx) {
+TCB_HD float tclamp(float x, float mn, float mx) {
     x = (x < mn) ? mn : x;
     return (x > mx) ? mx : x;
 }
@@ -44,7 +46,7 @@ struct LutPos {
     float w, w1;  // w, 1 - w
 };
 
-__device__ __forceinline__ LutPos lut_pos(float X, const Lut& L) {
+TCB_HD LutPos lut_pos(float X, const Lut& L) {
     X = tclamp(X, L.mn, L.mx);
     float f = (X - L.mn) * L.step;
     long long idx = (f != f) ? 0 : (long long)f;   // .to(torch.long) truncates
@@ -59,10 +61,18 @@ __device__ __forceinline__ LutPos lut_pos(float X, const Lut& L) {
     return p;
 }
 
+TCB_HD float ldro(const float* p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
 template <int NCOL>
-__device__ __forceinline__ float lut_col(const Lut& L, const LutPos& p, int c) {
+TCB_HD float lut_col(const Lut& L, const LutPos& p, int c) {
     const float* r0 = L.tab + (int64_t)p.lo * NCOL;
-    return p.w1 * __ldg(r0 + c) + p.w * __ldg(r0 + NCOL + c);
+    return p.w1 * ldro(r0 + c) + p.w * ldro(r0 + NCOL + c);
 }
 
 // host-side helpers describing a table the way the reference does

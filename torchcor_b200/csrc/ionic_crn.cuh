@@ -152,7 +152,7 @@ struct CRN {
     }
 
     // ------------------------------------------------------ tables (:212-328)
-    __device__ static void cai_row(float cai, const C& c, float* o) {
+    __host__ __device__ static void cai_row(float cai, const C& c, float* o) {
         float con = cai / 1000.0f;
         o[CC_conCa] = con;
         o[CC_carow_1] = sdiv(c.fGup_maxIup, 1.0f + sdiv(c.K_up, con));
@@ -163,7 +163,7 @@ struct CRN {
         o[CC_f_Ca_A] = (-f_Ca_inf) * c.f_Ca_C;
     }
 
-    __device__ static void fn_row(float fn, const C& c, float* o) {
+    __host__ __device__ static void fn_row(float fn, const C& c, float* o) {
         float eu = expf((3.4175e-13f - fn) / 13.67e-16f);
         float tau_v = sdiv(2.09f, 1.0f + eu) + 1.91f;
         float u_inf = sdiv(1.0f, 1.0f + eu);
@@ -174,18 +174,18 @@ struct CRN {
         o[1] = (-v_inf) * expm1f(e);
     }
 
-    __device__ static void rl_tau(float* o, int a_col, float inf, float tau, const C& c) {
+    __host__ __device__ static void rl_tau(float* o, int a_col, float inf, float tau, const C& c) {
         float e = sdiv(c.mdt, tau);
         o[a_col + 1] = expf(e);
         o[a_col] = (-inf) * expm1f(e);
     }
-    __device__ static void rl_ab(float* o, int a_col, float a, float b, const C& c) {
+    __host__ __device__ static void rl_ab(float* o, int a_col, float a, float b, const C& c) {
         float ab = a + b;
         o[a_col] = ((-a) / ab) * expm1f(ab * c.mdt);
         o[a_col + 1] = expf(ab * c.mdt);
     }
 
-    __device__ static void v_row(float V, const C& c, float* o) {
+    __host__ __device__ static void v_row(float V, const C& c, float* o) {
         o[CV_GKur] = sdiv(0.05f, 1.0f + expf((15.0f - V) / 13.0f)) + 0.005f;
         o[CV_IbNa] = c.GbNa * (V - c.E_Na);
         float a_h = (V >= -40.0f) ? 0.0f : 0.135f * expf(((V + 80.0f) - c.factorhGate) / -6.8f);
@@ -259,13 +259,13 @@ struct CRN {
         rl_tau(o, CV_xs_A, xs_inf, tau_xs, c);
     }
 
-    __device__ static void init(const C& c, float* s, float& V) {
+    __host__ __device__ static void init(const C& c, float* s, float& V) {
         for (int i = 0; i < CRN_NS; ++i) s[i] = c.init[i];
         V = c.V_init;
     }
 
     // ------------------------------------------------ differentiate (:358-444)
-    __device__ static float step(float V, float* s, const C& c, const Tables& T) {
+    __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
         LutPos pv = lut_pos(V, T.V);
         LutPos pc = lut_pos(s[R_Cai], T.Cai);
 #define VR(col) lut_col<CV_NCOL>(T.V, pv, col)

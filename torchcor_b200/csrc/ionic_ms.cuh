@@ -41,13 +41,13 @@ struct MS {
     static int64_t table_floats(const double*) { return 0; }
     static Tables tables(const float*, const double*) { return Tables{}; }
 
-    __device__ static void init(const C& c, float* s, float& V) {
+    __host__ __device__ static void init(const C& c, float* s, float& V) {
         s[0] = c.H_init;
         V = c.V_init;
     }
 
     // ModifiedMS2v.differentiate (:36-44); returns dU and updates H
-    __device__ static float step(float U, float* s, const C& c, const Tables&) {
+    __host__ __device__ static float step(float U, float* s, const C& c, const Tables&) {
         float H = s[0];
         float Uad = (U - c.vmin) / c.DV;
         float J_in = ((((-1.0f * H) * Uad) * (Uad - c.u_crit)) * (1.0f - Uad)) / c.tau_in;

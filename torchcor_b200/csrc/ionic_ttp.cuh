@@ -155,7 +155,7 @@ struct TTP {
     }
 
     // -------------------------------------------------------- tables (:197-318)
-    __device__ static void cass_row(float cs, const C& c, float* out) {
+    __host__ __device__ static void cass_row(float cs, const C& c, float* out) {
         float q = cs / 0.05f;
         float q2 = q * q;
         float FCaSS_inf = sdiv(0.6f, 1.0f + q2) + 0.4f;
@@ -166,7 +166,7 @@ struct TTP {
         out[1] = (-FCaSS_inf) * expm1f(e);
     }
 
-    __device__ static void v_row(float V, const C& c, float* o) {
+    __host__ __device__ static void v_row(float V, const C& c, float* o) {
         float D_inf = sdiv(1.0f, 1.0f + expf((c.D_off - V) / 7.5f));
         float F2_inf = sdiv(0.67f, 1.0f + expf((V + 35.0f) / 7.0f)) + 0.33f;
         float F_inf = sdiv(1.0f, 1.0f + expf((V + 20.0f) / 7.0f));
@@ -246,25 +246,25 @@ struct TTP {
         gate(o, TV_Xs_A, Xs_inf, tau_Xs, c);
     }
     // Rush-Larsen pair: B = exp(-dt/tau), A = -inf * expm1(-dt/tau)
-    __device__ static void gate(float* o, int a_col, float inf, float tau, const C& c) {
+    __host__ __device__ static void gate(float* o, int a_col, float inf, float tau, const C& c) {
         float e = sdiv(c.mdt, tau);
         o[a_col + 1] = expf(e);
         o[a_col] = (-inf) * expm1f(e);
     }
 
-    __device__ static float vek_row(float V) {
+    __host__ __device__ static float vek_row(float V) {
         float a_K1 = sdiv(0.1f, 1.0f + expf(0.06f * (V - 200.0f)));
         float b_K1 = ((3.0f * expf(0.0002f * (V + 100.0f))) + expf(0.1f * (V - 10.0f))) / (1.0f + expf(-0.5f * V));
         return a_K1 / (a_K1 + b_K1);
     }
 
-    __device__ static void init(const C& c, float* s, float& V) {
+    __host__ __device__ static void init(const C& c, float* s, float& V) {
         for (int i = 0; i < TTP_NS; ++i) s[i] = c.init[i];
         V = c.V_init;
     }
 
     // ---------------------------------------------------- differentiate (:353-454)
-    __device__ static float step(float V, float* s, const C& c, const Tables& T) {
+    __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
         LutPos pv = lut_pos(V, T.V);
         const float CaSR = s[S_CaSR], CaSS = s[S_CaSS], Cai = s[S_Cai], Ki = s[S_Ki], Nai = s[S_Nai];
         LutPos pc = lut_pos(CaSS, T.CaSS);

@@ -62,10 +62,10 @@ class Monodomain:
         """Mesh already in memory: nodes (N,3) in mm, elems (E,3|4), per-element regions and fibres."""
         self.n_nodes = int(nodes.shape[0])
         self._elems_np = np.ascontiguousarray(elems, dtype=np.int32)
-        self.nodes = torch.from_numpy(np.asarray(nodes)).to(dtype=torch.float32, device=self.device)
+        self.nodes = torch.from_numpy(np.ascontiguousarray(nodes)).to(dtype=torch.float32, device=self.device)
         self.elems = torch.from_numpy(self._elems_np).to(device=self.device)
         self.regions = torch.from_numpy(np.ascontiguousarray(regions)).to(dtype=torch.int, device=self.device)
-        self.fibres = torch.from_numpy(np.asarray(fibres)).to(dtype=torch.float32, device=self.device)
+        self.fibres = torch.from_numpy(np.ascontiguousarray(fibres)).to(dtype=torch.float32, device=self.device)
         self.stimuli = Stimuli(self.n_nodes, self.device, self.dtype)
         self.conductivity = Conductivity(self.regions, dtype=self.dtype)
 
