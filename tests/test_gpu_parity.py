@@ -58,7 +58,7 @@ def test_lookup_tables(lib, cuda, model, kw):
         if skip is not None:
             ok[skip] = True
         assert ok.all(), (np.nonzero(~ok)[0][:10], np.nonzero(~ok)[1][:10])
-        assert (got == p).mean() > 0.75
+        assert (got == p).mean() > 0.5
     assert off == t.size
 
 
