@@ -167,6 +167,18 @@ int tcb_mono_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* 
  * ms_ionic / ms_cg (for roofline accounting; costs one event pair per launch). */
 int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream, double* ms_ionic,
                      double* ms_cg);
+/* tcb_mono_run without scratch arguments (no counterpart in the reference):
+ * for callers that cannot allocate device memory at the call site (a host
+ * application that owns the device memory pool and forbids allocations after
+ * start-up, or a latency-critical caller that cannot afford cudaMalloc's
+ * implicit synchronisation).  The CG kernel's reduction partials and barrier
+ * words live in a static device array of the library (64 KiB + 16 B per GPU,
+ * held until exit); m->scratch and m->barrier are ignored.  Allocates nothing.
+ * The first call on a device looks up the array's address (make it before any
+ * stream capture).  Calls whose kernels overlap on the GPU share the array and
+ * race: serialise them.  A launch needing more than 2048 CG blocks is
+ * rejected with TCB_ERANGE. */
+int tcb_mono_run_noalloc(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream);
 /* Activation/repolarisation update and snapshot for the final step. */
 int tcb_mono_finish(const tcb_mono* m, void* stream);
 /* Device error word after a run (TCB_OK or TCB_ETIMEOUT); synchronises the stream. */

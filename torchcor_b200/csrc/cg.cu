@@ -268,6 +268,16 @@ DeviceInfo& device_info() {
 
 int num_sms() { return device_info().sms; }
 
+// Number of blocks launch_cg uses for this simulation on the current device.
+int cg_blocks(const MonoDev& d) {
+    DeviceInfo& di = device_info();
+    int64_t want = ceil_div(d.n_slices, kMinSlicesPerBlock);
+    int64_t cap = (int64_t)di.sms * di.cg_blocks_per_sm;
+    if (cap > kMaxBlocks) cap = kMaxBlocks;
+    int64_t nb = want < cap ? want : cap;
+    return (int)(nb < 1 ? 1 : nb);
+}
+
 int launch_cg(const MonoDev& d, cudaStream_t s) {
     DeviceInfo& di = device_info();
     if (di.cg_blocks_per_sm <= 0) return fail(TCB_ECUDA, "CG kernel cannot be resident on this device");
