@@ -82,10 +82,18 @@ int tcb_assemble_gather(int32_t k, const int32_t* slot_ptr, const int32_t* slot_
                         const float* ke, const float* mw, float* k_val, float* m_val, void* stream);
 /* Monodomain.assemble system values (monodomain.py:93-106, preconditioner.py:9-27):
  * k_val /= chi (in place); a_val = m*cm + (k*dt)*theta; k_rhs = ((1-theta)*dt)*k;
- * d_inv[i] = 1/a(i,i) (0 for i >= n_nodes up to n_pad). */
+ * d_inv[i] = 1/a(i,i) (0 for i >= n_nodes up to n_pad).  *a_split (device int32, caller sets 1)
+ * is cleared if any a_val differs from fp32(fp32(m*cm) + k_rhs); it stays 1 for theta = 0.5, and the
+ * solver then rebuilds A from M and k_rhs instead of streaming it. */
 int tcb_assemble_system(int64_t nnz, int64_t n_nodes, int64_t n_pad, const int32_t* diag, float* k_val,
                         const float* m_val, double chi, double cm, double dt, double theta,
-                        float* a_val, float* k_rhs, float* d_inv, void* stream);
+                        float* a_val, float* k_rhs, float* d_inv, int32_t* a_split, void* stream);
+/* int16 column offsets (col - row) of a sliced-ELL column array; *max_abs
+ * (device int32, caller-zeroed) receives max |col - row|.  The offsets are
+ * usable when that maximum is below 32768.  Replaces nothing in the
+ * reference (index compression of the solver's matrix stream). */
+int tcb_sell_delta(int64_t n_rows, const int64_t* slice_ptr, int64_t n_slices, const int32_t* sell_col,
+                   int16_t* delta, int32_t* max_abs, void* stream);
 /* Repack up to 4 CSR value arrays (and the columns) into sliced ELL; padding
  * entries get column = own row and value 0. */
 int tcb_sell_pack(int64_t n_rows, const int32_t* rowptr, const int32_t* col, const int64_t* slice_ptr,
@@ -123,6 +131,7 @@ typedef struct tcb_mono {
     /* matrix (sliced ELL, TCB_SLICE rows per slice) */
     const int64_t* slice_ptr;
     const int32_t* col;
+    const int16_t* col_delta; /* optional: col - row as int16 (all |col-row| < 32768), or NULL */
     const float* m_val;      /* M */
     const float* k_val;      /* ((1-theta)*dt) * K/chi */
     const float* a_val;      /* Cm*M + theta*dt*K/chi */
@@ -147,6 +156,7 @@ typedef struct tcb_mono {
     /* solver */
     double a_tol, r_tol;
     int32_t max_iter, linear_guess, at_rt, per_frame;
+    int32_t a_split;         /* 1 if every a_val == fp32(fp32(m_val*cm) + k_val) (tcb_assemble_system's check) */
     float cm, dt;
     /* device bookkeeping (caller-allocated, zero-initialised) */
     int32_t* step_iters;     /* [nt+1] CG iterations of each step */

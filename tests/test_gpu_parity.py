@@ -127,6 +127,10 @@ def test_assembly_matches_reference(lib, cuda, name, tmp_path):
     np.testing.assert_allclose(s.a_val.cpu().numpy(), A, rtol=1e-4, atol=2e-6 * np.abs(A).max())
     np.testing.assert_allclose(s.d_inv[: s.n].cpu().numpy(), g["PC"], rtol=1e-5)
     assert (s.d_inv[s.n:] == 0).all()
+    # theta = 0.5: A is exactly fp32(fp32(M*Cm) + ((1-theta)dt)K/chi), so the solver may rebuild it
+    assert s.a_split
+    rebuilt = s.m_val * np.float32(0.01) + s.krhs_val
+    assert torch.equal(rebuilt, s.a_val)
 
 
 # ------------------------------------------------------------------ whole solves
@@ -153,6 +157,15 @@ def test_monodomain_matches_reference(lib, cuda, name, tmp_path):
     assert err <= 1e-3, err
     ref_total = int(g["n_total_iter"])
     assert abs(total - ref_total) <= max(3, ref_total // 50), (total, ref_total)
+
+
+@pytest.mark.parametrize("variant", [dict(TCB_CG_KERNEL="streaming"), dict(TCB_CG_INDEX="int32")])
+@pytest.mark.parametrize("name", ["cube8_ttp_f32", "ico3_crn_f32", "cube4_ms_rt_f32"])
+def test_monodomain_cg_variants(lib, cuda, name, variant, tmp_path, monkeypatch):
+    """The CG paths large meshes take (streaming kernel; 32-bit column stream)."""
+    for k, v in variant.items():
+        monkeypatch.setenv(k, v)
+    test_monodomain_matches_reference(lib, cuda, name, tmp_path)
 
 
 @pytest.mark.parametrize("name,ref64", [("cfg1_ms_f32", "cfg1_ms_f64"), ("cube8_ttp_f32", "cube8_ttp_f64"),

@@ -36,13 +36,13 @@ class tcb_mono(C.Structure):
     _fields_ = [
         ("n_nodes", _i64), ("n_pad", _i64), ("n_slices", _i64), ("nt", _i64),
         ("model", _i32), ("n_states", _i32),
-        ("slice_ptr", _vp), ("col", _vp), ("m_val", _vp), ("k_val", _vp), ("a_val", _vp), ("d_inv", _vp),
+        ("slice_ptr", _vp), ("col", _vp), ("col_delta", _vp), ("m_val", _vp), ("k_val", _vp), ("a_val", _vp), ("d_inv", _vp),
         ("state", _vp), ("tables", _vp),
         ("x", _vp), ("bprime", _vp), ("r", _vp), ("p", _vp), ("ap", _vp), ("at", _vp), ("rt", _vp),
         ("snapshots", _vp),
         ("stim_bits", _vp), ("step_t", _vp), ("step_stim", _vp), ("stim_amp", C.c_float * TCB_MAX_STIMULI),
         ("a_tol", _f64), ("r_tol", _f64),
-        ("max_iter", _i32), ("linear_guess", _i32), ("at_rt", _i32), ("per_frame", _i32),
+        ("max_iter", _i32), ("linear_guess", _i32), ("at_rt", _i32), ("per_frame", _i32), ("a_split", _i32),
         ("cm", C.c_float), ("dt", C.c_float),
         ("step_iters", _vp), ("counter", _vp), ("scratch", _vp), ("barrier", _vp),
         ("params", _vp),
@@ -59,7 +59,9 @@ SIGNATURES = [
     ("tcb_sell_layout", C.c_int, [_vp, _i64, _vp, _pi64]),
     ("tcb_assemble_local", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("tcb_assemble_gather", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
-    ("tcb_assemble_system", C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp, _vp]),
+    ("tcb_assemble_system", C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp, _vp,
+                                      _vp]),
+    ("tcb_sell_delta", C.c_int, [_i64, _vp, _i64, _vp, _vp, _vp, _vp]),
     ("tcb_sell_pack", C.c_int, [_i64, _vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp]),
     ("tcb_model_params", C.c_char_p, [_i32]),
     ("tcb_model_states", C.c_char_p, [_i32]),

@@ -87,6 +87,8 @@ class System:
     sell_m: torch.Tensor
     sell_k: torch.Tensor
     sell_a: torch.Tensor
+    sell_dcol: torch.Tensor = None   # int16 col - row, or None
+    a_split: bool = False            # every A value == fp32(fp32(M*Cm) + K')
 
     def csr(self, values):
         return torch.sparse_csr_tensor(self.rowptr, self.col, values, size=(self.n, self.n))
@@ -114,8 +116,9 @@ def assemble_system(nodes, elems_np, sl, st, fibres, dt, chi=140, cm=0.01, theta
     a_val = torch.empty(nnz, device=dev, dtype=torch.float32)
     krhs = torch.empty(nnz, device=dev, dtype=torch.float32)
     d_inv = torch.empty(n_pad, device=dev, dtype=torch.float32)
+    a_split = torch.ones(1, device=dev, dtype=torch.int32)
     check(lib.tcb_assemble_system(nnz, n, n_pad, ptr(diag), ptr(k_val), ptr(m_val), float(chi), float(cm), float(dt),
-                                  float(theta), ptr(a_val), ptr(krhs), ptr(d_inv), s))
+                                  float(theta), ptr(a_val), ptr(krhs), ptr(d_inv), ptr(a_split), s))
     # sliced ELL
     n_slices = (n + _lib.TCB_SLICE - 1) // _lib.TCB_SLICE
     sp = np.empty(n_slices + 1, dtype=np.int64)
@@ -130,9 +133,15 @@ def assemble_system(nodes, elems_np, sl, st, fibres, dt, chi=140, cm=0.01, theta
     vin = (C.c_void_p * 3)(ptr(m_val), ptr(krhs), ptr(a_val))
     vout = (C.c_void_p * 3)(*[ptr(t) for t in sell])
     check(lib.tcb_sell_pack(n, ptr(rowptr), ptr(col), ptr(slice_ptr), n_slices, 3, vin, ptr(sell_col), vout, s))
+    # int16 column offsets when the mesh ordering keeps every |col - row| < 32768
+    dcol = torch.empty(ne, device=dev, dtype=torch.int16)
+    mx = torch.zeros(1, device=dev, dtype=torch.int32)
+    check(lib.tcb_sell_delta(n, ptr(slice_ptr), n_slices, ptr(sell_col), ptr(dcol), ptr(mx), s))
+    if int(mx.item()) >= 32768:
+        dcol = None
     return System(n=n, n_pad=n_pad, nnz=nnz, rowptr=rowptr, col=col, m_val=m_val, k_val=k_val, a_val=a_val,
                   krhs_val=krhs, d_inv=d_inv, n_slices=n_slices, slice_ptr=slice_ptr, sell_col=sell_col,
-                  sell_m=sell[0], sell_k=sell[1], sell_a=sell[2])
+                  sell_m=sell[0], sell_k=sell[1], sell_a=sell[2], sell_dcol=dcol, a_split=bool(a_split.item()))
 
 
 class _Matrices:

@@ -34,6 +34,7 @@ MonoDev make_dev(const tcb_mono* m) {
     d.nt = m->nt;
     d.slice_ptr = m->slice_ptr;
     d.col = m->col;
+    d.dcol = m->col_delta;
     d.mv = m->m_val;
     d.kv = m->k_val;
     d.av = m->a_val;
@@ -60,6 +61,7 @@ MonoDev make_dev(const tcb_mono* m) {
     d.linear_guess = m->linear_guess;
     d.at_rt = m->at_rt;
     d.per_frame = m->per_frame;
+    d.a_split = m->a_split;
     d.cm = m->cm;
     d.dt = m->dt;
     for (int k = 0; k < TCB_MAX_STIMULI; ++k) d.amp[k] = m->stim_amp[k];

@@ -173,13 +173,17 @@ __global__ void gather_kernel(const int32_t* __restrict__ slot_ptr, const int32_
 
 __global__ void system_kernel(int64_t nnz, float* __restrict__ kval, const float* __restrict__ mval, float chi,
                               float cm, float dt, float theta, float rhs_scale, float* __restrict__ aval,
-                              float* __restrict__ krhs) {
+                              float* __restrict__ krhs, int32_t* a_split) {
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nnz) return;
     float k = __fdiv_rn(kval[s], chi);                                    // K / chi   (monodomain.py:93)
     kval[s] = k;
-    aval[s] = __fadd_rn(__fmul_rn(mval[s], cm), __fmul_rn(__fmul_rn(k, dt), theta));  // :96
-    krhs[s] = __fmul_rn(k, rhs_scale);                                     // ((1-theta)*dt)*K  (:131)
+    const float mc = __fmul_rn(mval[s], cm);
+    const float a = __fadd_rn(mc, __fmul_rn(__fmul_rn(k, dt), theta));  // :96
+    const float kr = __fmul_rn(k, rhs_scale);                             // ((1-theta)*dt)*K  (:131)
+    aval[s] = a;
+    krhs[s] = kr;
+    if (a_split && __fadd_rn(mc, kr) != a) atomicAnd(a_split, 0);
 }
 
 __global__ void jacobi_kernel(int64_t n, int64_t n_pad, const int32_t* __restrict__ diag,
@@ -217,6 +221,26 @@ __global__ void sell_pack_kernel(int64_t n_rows, int64_t n_slices, const int32_t
     }
 }
 
+__global__ void sell_delta_kernel(int64_t n_rows, int64_t n_slices, const int64_t* __restrict__ slice_ptr,
+                                  const int32_t* __restrict__ scol, int16_t* __restrict__ delta, int32_t* max_abs) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t s = t / TCB_SLICE;
+    int lane = (int)(t % TCB_SLICE);
+    if (s >= n_slices) return;
+    int64_t row = s * TCB_SLICE + lane;
+    int64_t base = slice_ptr[s];
+    int32_t w = (int32_t)((slice_ptr[s + 1] - base) / TCB_SLICE);
+    int32_t m = 0;
+    for (int32_t k = 0; k < w; ++k) {
+        int64_t e = base + (int64_t)k * TCB_SLICE + lane;
+        int64_t dlt = row < n_rows ? (int64_t)scol[e] - row : 0;
+        int64_t a = dlt < 0 ? -dlt : dlt;
+        if (a > m) m = a > INT32_MAX ? INT32_MAX : (int32_t)a;
+        delta[e] = (int16_t)(a < 32768 ? dlt : 0);
+    }
+    atomicMax(max_abs, m);   // integer maximum: order-independent
+}
+
 inline unsigned blocks_for(int64_t n) { return (unsigned)tcb::ceil_div(n, kThreads); }
 
 }  // namespace
@@ -249,16 +273,27 @@ extern "C" int tcb_assemble_gather(int32_t k, const int32_t* slot_ptr, const int
 
 extern "C" int tcb_assemble_system(int64_t nnz, int64_t n, int64_t n_pad, const int32_t* diag, float* k_val,
                                    const float* m_val, double chi, double cm, double dt, double theta, float* a_val,
-                                   float* k_rhs, float* d_inv, void* stream) {
+                                   float* k_rhs, float* d_inv, int32_t* a_split, void* stream) {
     if (!diag || !k_val || !m_val || !a_val || !k_rhs || !d_inv || nnz <= 0 || n <= 0 || n_pad < n)
         return tcb::fail(TCB_EINVAL, "tcb_assemble_system: bad arguments");
     cudaStream_t s = tcb::as_stream(stream);
     // Python-level scalars meet float32 tensors: each is rounded to float32 first
     system_kernel<<<blocks_for(nnz), kThreads, 0, s>>>(nnz, k_val, m_val, (float)chi, (float)cm, (float)dt,
-                                                        (float)theta, (float)((1.0 - theta) * dt), a_val, k_rhs);
+                                                        (float)theta, (float)((1.0 - theta) * dt), a_val, k_rhs,
+                                                        a_split);
     TCB_CHECK_LAUNCH("system kernel");
     jacobi_kernel<<<blocks_for(n_pad), kThreads, 0, s>>>(n, n_pad, diag, a_val, d_inv);
     TCB_CHECK_LAUNCH("jacobi kernel");
+    return TCB_OK;
+}
+
+extern "C" int tcb_sell_delta(int64_t n_rows, const int64_t* slice_ptr, int64_t n_slices, const int32_t* sell_col,
+                              int16_t* delta, int32_t* max_abs, void* stream) {
+    if (!slice_ptr || !sell_col || !delta || !max_abs || n_rows <= 0 || n_slices != tcb::ceil_div(n_rows, TCB_SLICE))
+        return tcb::fail(TCB_EINVAL, "tcb_sell_delta: bad arguments");
+    sell_delta_kernel<<<blocks_for(n_slices * TCB_SLICE), kThreads, 0, tcb::as_stream(stream)>>>(
+        n_rows, n_slices, slice_ptr, sell_col, delta, max_abs);
+    TCB_CHECK_LAUNCH("sell delta kernel");
     return TCB_OK;
 }
 

@@ -13,118 +13,20 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include <mutex>
 #include <vector>
 
+#include "cg_common.cuh"
 #include "mono.cuh"
 #include "tcb_internal.h"
 
 namespace tcb {
 namespace {
 
-constexpr int kCgThreads = 512;
-constexpr int kCgWarps = kCgThreads / 32;
-constexpr int kMinSlicesPerBlock = 2 * kCgWarps;
-constexpr int kMaxBlocks = 2048;
-constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;  // 2 s: a wait that long means a lost block
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ uint64_t globaltimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Grid-wide barrier with a bounded wait: returns false (and the kernel must
-// return) if any block recorded an error or the wait ran past the timeout.
-__device__ bool grid_barrier(uint32_t* bar, int32_t* err) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int good = 1;
-        const unsigned gen = ld_acquire(bar + 1);
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const uint64_t t0 = globaltimer();
-            while (ld_acquire(bar + 1) == gen) {
-                if (*(volatile int32_t*)err != 0) {
-                    good = 0;
-                    break;
-                }
-                if (globaltimer() - t0 > kBarrierTimeoutNs) {
-                    atomicCAS(err, 0, TCB_ETIMEOUT);
-                    good = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        if (*(volatile int32_t*)err != 0) good = 0;
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
-// Block partial of NV float64 values -> parts[blockIdx.x * NV + i] (fixed order).
-template <int NV>
-__device__ void block_partial(double (&v)[NV], double* parts, double* sh) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-        double t = warp_sum(v[i]);
-        if (lane == 0) sh[warp * NV + i] = t;
-    }
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            double t = lane < kCgWarps ? sh[lane * NV + i] : 0.0;
-            t = warp_sum(t);
-            if (lane == 0) parts[blockIdx.x * NV + i] = t;
-        }
-    }
-}
-
-// Sum of all blocks' partials; every block computes the same value.
-template <int NV>
-__device__ void grid_total(const double* parts, double (&out)[NV], double* sh) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == 0) {
-        double acc[NV];
-#pragma unroll
-        for (int i = 0; i < NV; ++i) acc[i] = 0.0;
-        for (unsigned b = lane; b < gridDim.x; b += 32)
-#pragma unroll
-            for (int i = 0; i < NV; ++i) acc[i] += __ldcg(parts + b * NV + i);
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            acc[i] = warp_sum(acc[i]);
-            if (lane == 0) sh[i] = acc[i];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < NV; ++i) out[i] = sh[i];
-}
+using namespace cgk;
 
 __global__ void __launch_bounds__(kCgThreads) cg_kernel(MonoDev d) {
     __shared__ double sh_part[kCgWarps * 2];
@@ -268,8 +170,17 @@ DeviceInfo& device_info() {
 
 int num_sms() { return device_info().sms; }
 
+// TCB_CG_KERNEL=streaming forces the streaming kernel, TCB_CG_INDEX=int32 the
+// 32-bit column stream (both for testing the paths large meshes take).
+static bool env_is(const char* name, const char* value) {
+    const char* v = getenv(name);
+    return v && strcmp(v, value) == 0;
+}
+
 // Number of blocks launch_cg uses for this simulation on the current device.
 int cg_blocks(const MonoDev& d) {
+    int r = env_is("TCB_CG_KERNEL", "streaming") ? 0 : resident_blocks(d);
+    if (r > 0) return r;
     DeviceInfo& di = device_info();
     int64_t want = ceil_div(d.n_slices, kMinSlicesPerBlock);
     int64_t cap = (int64_t)di.sms * di.cg_blocks_per_sm;
@@ -279,6 +190,13 @@ int cg_blocks(const MonoDev& d) {
 }
 
 int launch_cg(const MonoDev& d, cudaStream_t s) {
+    if (!env_is("TCB_CG_KERNEL", "streaming")) {
+        MonoDev dd = d;
+        if (env_is("TCB_CG_INDEX", "int32")) dd.dcol = nullptr;
+        int r = launch_cg_resident(dd, s);
+        if (r < 0) return r;
+        if (r == 1) return TCB_OK;
+    }
     DeviceInfo& di = device_info();
     if (di.cg_blocks_per_sm <= 0) return fail(TCB_ECUDA, "CG kernel cannot be resident on this device");
     int64_t want = ceil_div(d.n_slices, kMinSlicesPerBlock);

@@ -10,6 +10,7 @@ struct MonoDev {
     int64_t n, n_pad, n_slices, nt;
     const int64_t* slice_ptr;
     const int32_t* col;
+    const int16_t* dcol;   // int16 column offsets from the row, or null
     const float *mv, *kv, *av, *dinv;
     float* state;
     float *x, *bp, *r, *p, *ap, *at, *rt, *snap;
@@ -22,6 +23,7 @@ struct MonoDev {
     uint32_t* bar;
     double a_tol, r_tol;
     int32_t max_iter, linear_guess, at_rt, per_frame;
+    int32_t a_split;   // A == fp32(fp32(M*Cm) + K') verified at assembly
     float cm, dt;
     float amp[TCB_MAX_STIMULI];
 };
@@ -37,5 +39,7 @@ __host__ __device__ inline int64_t ring_next(int64_t n) { return n % 3; }
 int launch_mono_ionic(const tcb_mono* m, const MonoDev& d, cudaStream_t s);
 int launch_mono_finish(const MonoDev& d, cudaStream_t s);
 int launch_cg(const MonoDev& d, cudaStream_t s);
+int launch_cg_resident(const MonoDev& d, cudaStream_t s);
+int resident_blocks(const MonoDev& d);
 
 }  // namespace tcb

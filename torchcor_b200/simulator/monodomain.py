@@ -122,7 +122,7 @@ class Monodomain:
         m = _lib.tcb_mono()
         m.n_nodes, m.n_pad, m.n_slices, m.nt = n, n_pad, s.n_slices, nt
         m.model, m.n_states = im.model_id, im.state.shape[0]
-        m.slice_ptr, m.col = ptr(s.slice_ptr), ptr(s.sell_col)
+        m.slice_ptr, m.col, m.col_delta = ptr(s.slice_ptr), ptr(s.sell_col), ptr(s.sell_dcol)
         m.m_val, m.k_val, m.a_val, m.d_inv = ptr(s.sell_m), ptr(s.sell_k), ptr(s.sell_a), ptr(s.d_inv)
         m.state, m.tables = ptr(im.state), ptr(im.tables)
         m.x, m.bprime, m.r, m.p, m.ap = (ptr(sim[k]) for k in ("x", "bp", "r", "p", "ap"))
@@ -134,6 +134,7 @@ class Monodomain:
         m.a_tol, m.r_tol, m.max_iter = float(a_tol), float(r_tol), int(max_iter)
         m.linear_guess, m.at_rt, m.per_frame = int(bool(linear_guess)), int(bool(calculate_AT_RT)), per_frame
         m.cm, m.dt = float(self.Cm), float(self.dt)
+        m.a_split = int(s.a_split)
         m.step_iters, m.counter = ptr(sim["step_iters"]), ptr(sim["counter"])
         m.scratch, m.barrier = ptr(sim["scratch"]), ptr(sim["barrier"])
         m.params = sim["params"].ctypes.data
