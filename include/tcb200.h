@@ -111,6 +111,12 @@ int tcb_sell_pack(int64_t n_rows, const int32_t* rowptr, const int32_t* col, con
 const char* tcb_model_params(int32_t model);       /* comma-separated parameter names */
 const char* tcb_model_states(int32_t model);       /* comma-separated state names (row order) */
 int tcb_model_layout(int32_t model, const double* params, int64_t* n_states, int64_t* table_floats);
+/* Layout of lookup table `index` (0, 1, 2 in the reference's construction
+ * order: TTP V, CaSS, V-Ek; CRN Cai... listed as V, Cai, fn) inside the model's
+ * table array: rows x stride floats (stride = ncol rounded up to 4, or 1)
+ * starting at float offset `offset`.  TCB_ERANGE past the last table. */
+int tcb_model_table_info(int32_t model, int32_t index, int64_t* rows, int32_t* ncol, int32_t* stride,
+                         int64_t* offset);
 /* construct_tables (TTP :197-318, CRN :212-328); no-op for MS */
 int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream);
 /* initialize(n_nodes): fill state rows and V with the initial values */

@@ -69,10 +69,18 @@ def test_table_sizes_match_reference_arange(lib):
     m = ionic.TenTusscherPanfilov("ENDO", 0.01, device="cpu")
     lib.tcb_model_layout(2, m.param_array().ctypes.data, C.byref(ns), C.byref(nt))
     rows = lambda a, b, r: torch.arange(a, b, r).shape[0]  # noqa: E731
-    assert nt.value == rows(-800., 800., 0.05) * 27 + rows(0.00001, 10.0, 0.00001) * 3 + rows(-800., 800., 0.05)
+    from torchcor_b200 import _lib
+    lay = _lib.table_layout(2)
+    assert [(r, c) for r, c, _, _ in lay] == [(rows(-800., 800., 0.05), 27), (rows(0.00001, 10.0, 0.00001), 3),
+                                             (rows(-800., 800., 0.05), 1)]
+    assert [st for _, _, st, _ in lay] == [28, 4, 1]
+    assert nt.value == sum(r * st for r, _, st, _ in lay)
     m = ionic.CourtemancheRamirezNattel(0.02, device="cpu")
     lib.tcb_model_layout(3, m.param_array().ctypes.data, C.byref(ns), C.byref(nt))
-    assert nt.value == rows(-200., 200., 0.1) * 32 + rows(3e-4, 30.0, 3e-4) * 5 + rows(-2e-11, 10.0e-11, 2e-15) * 3
+    lay = _lib.table_layout(3)
+    assert [(r, c) for r, c, _, _ in lay] == [(rows(-200., 200., 0.1), 32), (rows(3e-4, 30.0, 3e-4), 5),
+                                             (rows(-2e-11, 10.0e-11, 2e-15), 3)]
+    assert nt.value == sum(r * st for r, _, st, _ in lay)
 
 
 @pytest.mark.parametrize("name", ["cube6_ms_f32", "cfg1_ms_f32", "cube8_ttp_f32", "ico3_crn_f32",

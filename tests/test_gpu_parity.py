@@ -46,11 +46,15 @@ def test_lookup_tables(lib, cuda, model, kw):
         for a in CRN_SINGULAR:
             near |= np.abs(grid - a) < 0.15
         parts = [(ref.V_tab, near), (ref.Cai_tab, None), (ref.fn_tab, None)]
-    off = 0
-    for p, skip in parts:
+    from torchcor_b200 import _lib
+    layout = _lib.table_layout(dev.model_id)
+    assert len(layout) == len(parts)
+    for (p, skip), (rows, ncol, stride, off) in zip(parts, layout):
         p = p.numpy()
-        got = t[off:off + p.size].reshape(p.shape)
-        off += p.size
+        assert p.shape == (rows, ncol)
+        padded = t[off:off + rows * stride].reshape(rows, stride)
+        assert (padded[:, ncol:] == 0).all()
+        got = padded[:, :ncol]
         assert np.isfinite(got).all()
         # same float32 grid as torch.arange; exp/log/expm1 differ by a few ulp
         tol = 1e-5 * np.abs(p) + 1e-7 * np.abs(p).max(axis=0)
@@ -59,7 +63,7 @@ def test_lookup_tables(lib, cuda, model, kw):
             ok[skip] = True
         assert ok.all(), (np.nonzero(~ok)[0][:10], np.nonzero(~ok)[1][:10])
         assert (got == p).mean() > 0.5
-    assert off == t.size
+    assert layout[-1][3] + layout[-1][0] * layout[-1][2] == t.size
 
 
 # ------------------------------------------------------------------ one differentiate() call

@@ -66,6 +66,7 @@ SIGNATURES = [
     ("tcb_model_params", C.c_char_p, [_i32]),
     ("tcb_model_states", C.c_char_p, [_i32]),
     ("tcb_model_layout", C.c_int, [_i32, _vp, _pi64, _pi64]),
+    ("tcb_model_table_info", C.c_int, [_i32, _i32, _pi64, C.POINTER(_i32), C.POINTER(_i32), _pi64]),
     ("tcb_model_tables", C.c_int, [_i32, _vp, _vp, _vp]),
     ("tcb_model_init", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp]),
     ("tcb_model_differentiate", C.c_int, [_i32, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp]),
@@ -135,6 +136,18 @@ def stream_ptr(stream=None):
 
 def model_params(model):
     return load().tcb_model_params(model).decode().split(",")
+
+
+def table_layout(model):
+    """[(rows, ncol, stride, offset)] of the model's lookup tables."""
+    lib = load()
+    out = []
+    for i in range(3):
+        r, c, st, off = C.c_int64(), C.c_int32(), C.c_int32(), C.c_int64()
+        if lib.tcb_model_table_info(model, i, C.byref(r), C.byref(c), C.byref(st), C.byref(off)) != TCB_OK:
+            break
+        out.append((r.value, c.value, st.value, off.value))
+    return out
 
 
 def model_states(model):

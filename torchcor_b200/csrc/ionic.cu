@@ -66,14 +66,16 @@ __global__ void ttp_v_table(TTP::C c, float* tab, int64_t rows, double mn, doubl
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[TV_NCOL];
         TTP::v_row(grid_value(mn, res, i, rows), c, o);
-        for (int k = 0; k < TV_NCOL; ++k) tab[i * TV_NCOL + k] = o[k];
+        constexpr int S = lut_stride(TV_NCOL);
+        for (int k = 0; k < S; ++k) tab[i * S + k] = k < TV_NCOL ? o[k] : 0.0f;
     }
 }
 __global__ void ttp_cass_table(TTP::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[3];
         TTP::cass_row(grid_value(mn, res, i, rows), c, o);
-        for (int k = 0; k < 3; ++k) tab[i * 3 + k] = o[k];
+        constexpr int S = lut_stride(3);
+        for (int k = 0; k < S; ++k) tab[i * S + k] = k < 3 ? o[k] : 0.0f;
     }
 }
 __global__ void ttp_vek_table(float* tab, int64_t rows, double mn, double res) {
@@ -84,21 +86,24 @@ __global__ void crn_v_table(CRN::C c, float* tab, int64_t rows, double mn, doubl
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[CV_NCOL];
         CRN::v_row(grid_value(mn, res, i, rows), c, o);
-        for (int k = 0; k < CV_NCOL; ++k) tab[i * CV_NCOL + k] = o[k];
+        constexpr int S = lut_stride(CV_NCOL);
+        for (int k = 0; k < S; ++k) tab[i * S + k] = k < CV_NCOL ? o[k] : 0.0f;
     }
 }
 __global__ void crn_cai_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[CC_NCOL];
         CRN::cai_row(grid_value(mn, res, i, rows), c, o);
-        for (int k = 0; k < CC_NCOL; ++k) tab[i * CC_NCOL + k] = o[k];
+        constexpr int S = lut_stride(CC_NCOL);
+        for (int k = 0; k < S; ++k) tab[i * S + k] = k < CC_NCOL ? o[k] : 0.0f;
     }
 }
 __global__ void crn_fn_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
         float o[3];
         CRN::fn_row(grid_value(mn, res, i, rows), c, o);
-        for (int k = 0; k < 3; ++k) tab[i * 3 + k] = o[k];
+        constexpr int S = lut_stride(3);
+        for (int k = 0; k < S; ++k) tab[i * S + k] = k < 3 ? o[k] : 0.0f;
     }
 }
 
@@ -277,6 +282,31 @@ extern "C" int tcb_model_layout(int32_t model, const double* params, int64_t* n_
             return TCB_OK;
     }
     return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+extern "C" int tcb_model_table_info(int32_t model, int32_t index, int64_t* rows, int32_t* ncol, int32_t* stride,
+                                    int64_t* offset) {
+    if (!rows || !ncol || !stride || !offset) return fail(TCB_EINVAL, "tcb_model_table_info: null output");
+    const LutSpec* specs[3] = {nullptr, nullptr, nullptr};
+    if (model == TCB_MODEL_TTP) {
+        specs[0] = &TTP::kV;
+        specs[1] = &TTP::kCaSS;
+        specs[2] = &TTP::kVEk;
+    } else if (model == TCB_MODEL_CRN) {
+        specs[0] = &CRN::kV;
+        specs[1] = &CRN::kCai;
+        specs[2] = &CRN::kFn;
+    } else if (model != TCB_MODEL_MS) {
+        return fail(TCB_EINVAL, "unknown ionic model");
+    }
+    if (index < 0 || index > 2 || !specs[index]) return fail(TCB_ERANGE, "no such lookup table");
+    int64_t off = 0;
+    for (int i = 0; i < index; ++i) off += specs[i]->floats();
+    *rows = specs[index]->rows();
+    *ncol = specs[index]->ncol;
+    *stride = specs[index]->stride();
+    *offset = off;
+    return TCB_OK;
 }
 
 extern "C" int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream) {

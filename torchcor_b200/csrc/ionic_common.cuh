@@ -36,7 +36,7 @@ TCB_HD float tclamp(float x, float mn, float mx) {
 // Lookup table with the reference's linear interpolation
 // (TenTusscherPanfilov.py:188-195, CourtemancheRamirezNattel.py:203-210).
 struct Lut {
-    const float* tab;   // rows x ncol, row-major
+    const float* tab;   // rows x stride floats, row-major (stride = ncol rounded up to 4, or 1)
     float mn, mx, res, step;
     int32_t mx_idx;
 };
@@ -48,10 +48,10 @@ struct LutPos {
 
 TCB_HD LutPos lut_pos(float X, const Lut& L) {
     X = tclamp(X, L.mn, L.mx);
-    float f = (X - L.mn) * L.step;
-    long long idx = (f != f) ? 0 : (long long)f;   // .to(torch.long) truncates
+    float f = (X - L.mn) * L.step;   // X is clamped, so 0 <= f <= rows: 32-bit is enough
+    int idx = (f != f) ? 0 : (int)f;  // .to(torch.long) truncates
     idx = idx < 0 ? 0 : idx;
-    idx = idx > (long long)(L.mx_idx - 1) ? (long long)(L.mx_idx - 1) : idx;
+    idx = idx > L.mx_idx - 1 ? L.mx_idx - 1 : idx;
     float lo_pos = (float)idx * L.res + L.mn;
     float w = (X - lo_pos) / L.res;
     LutPos p;
@@ -69,16 +69,44 @@ TCB_HD float ldro(const float* p) {
 #endif
 }
 
+__host__ __device__ constexpr int lut_stride(int ncol) { return ncol == 1 ? 1 : (ncol + 3) / 4 * 4; }
+
+// one column of the interpolated row: (1 - w) * T[lo] + w * T[lo + 1]
 template <int NCOL>
 TCB_HD float lut_col(const Lut& L, const LutPos& p, int c) {
-    const float* r0 = L.tab + (int64_t)p.lo * NCOL;
-    return p.w1 * ldro(r0 + c) + p.w * ldro(r0 + NCOL + c);
+    constexpr int S = lut_stride(NCOL);
+    const float* r0 = L.tab + (int64_t)p.lo * S;
+    return p.w1 * ldro(r0 + c) + p.w * ldro(r0 + S + c);
+}
+
+// every column of the interpolated row, the two table rows read as 16-byte vectors
+template <int NCOL>
+TCB_HD void lut_row(const Lut& L, const LutPos& p, float* out) {
+    constexpr int S = lut_stride(NCOL);
+    static_assert(S % 4 == 0, "vector rows need a stride that is a multiple of 4");
+    const float* r0 = L.tab + (int64_t)p.lo * S;
+#ifdef __CUDA_ARCH__
+    float a[S], b[S];
+#pragma unroll
+    for (int q = 0; q < S / 4; ++q) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(r0) + q);
+        const float4 y = __ldg(reinterpret_cast<const float4*>(r0 + S) + q);
+        a[4 * q] = x.x; a[4 * q + 1] = x.y; a[4 * q + 2] = x.z; a[4 * q + 3] = x.w;
+        b[4 * q] = y.x; b[4 * q + 1] = y.y; b[4 * q + 2] = y.z; b[4 * q + 3] = y.w;
+    }
+#pragma unroll
+    for (int c = 0; c < NCOL; ++c) out[c] = p.w1 * a[c] + p.w * b[c];
+#else
+    for (int c = 0; c < NCOL; ++c) out[c] = p.w1 * r0[c] + p.w * r0[S + c];
+#endif
 }
 
 // host-side helpers describing a table the way the reference does
 struct LutSpec {
     double mn, mx, res;
     int ncol;
+    int stride() const { return lut_stride(ncol); }
+    int64_t floats() const { return rows() * stride(); }
     int64_t rows() const;       // torch.arange(mn, mx, res).shape[0]
     int32_t mx_idx() const;     // int((mx - mn) * (1/res)) - 1
     Lut make(const float* tab) const;

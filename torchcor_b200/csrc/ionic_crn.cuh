@@ -141,13 +141,13 @@ struct CRN {
     }
 
     static int64_t table_floats(const double*) {
-        return kV.rows() * kV.ncol + kCai.rows() * kCai.ncol + kFn.rows() * kFn.ncol;
+        return kV.floats() + kCai.floats() + kFn.floats();
     }
     static Tables tables(const float* t, const double*) {
         Tables T;
         T.V = kV.make(t);
-        T.Cai = kCai.make(t + kV.rows() * kV.ncol);
-        T.Fn = kFn.make(t + kV.rows() * kV.ncol + kCai.rows() * kCai.ncol);
+        T.Cai = kCai.make(t + kV.floats());
+        T.Fn = kFn.make(t + kV.floats() + kCai.floats());
         return T;
     }
 

@@ -144,13 +144,13 @@ struct TTP {
     }
 
     static int64_t table_floats(const double*) {
-        return kV.rows() * kV.ncol + kCaSS.rows() * kCaSS.ncol + kVEk.rows() * kVEk.ncol;
+        return kV.floats() + kCaSS.floats() + kVEk.floats();
     }
     static Tables tables(const float* t, const double*) {
         Tables T;
         T.V = kV.make(t);
-        T.CaSS = kCaSS.make(t + kV.rows() * kV.ncol);
-        T.VEk = kVEk.make(t + kV.rows() * kV.ncol + kCaSS.rows() * kCaSS.ncol);
+        T.CaSS = kCaSS.make(t + kV.floats());
+        T.VEk = kVEk.make(t + kV.floats() + kCaSS.floats());
         return T;
     }
 
