@@ -151,6 +151,8 @@ typedef struct tcb_mono {
     float* r;
     float* p;
     float* ap;
+    float* z;                /* batch solver only: z = D r of every row, n_pad */
+    float* p2;               /* batch solver only: second search-direction buffer, n_pad */
     float* at;
     float* rt;
     float* snapshots;        /* row j = solution of step j*per_frame, n_nodes per row; may be NULL */
@@ -199,6 +201,34 @@ int tcb_mono_run_noalloc(const tcb_mono* m, int64_t step_begin, int64_t step_end
 int tcb_mono_finish(const tcb_mono* m, void* stream);
 /* Device error word after a run (TCB_OK or TCB_ETIMEOUT); synchronises the stream. */
 int tcb_mono_check(const tcb_mono* m, void* stream);
+
+/* ---------------------------------------------------------------- batches
+ * Many simulations stepping together (no counterpart in the reference, which
+ * runs one simulation per process): one ionic launch per model and one
+ * persistent CG launch per step cover every simulation; each keeps its own
+ * arrays (a tcb_mono each, with the z and p2 buffers set), step counter,
+ * schedule, tolerances and iteration count (per-simulation convergence).
+ * Simulations may be at different steps; one whose counter is outside
+ * [1, nt] is skipped.  The plan is rebuilt (tcb_batch_prepare) whenever the
+ * set of simulations changes; the workspace is caller-allocated device memory
+ * of tcb_batch_workspace_bytes(n) bytes (n <= 1024).
+ */
+typedef struct tcb_batch_plan {
+    void* workspace;
+    int32_t n_sims, cg_blocks, cg_smem, n_groups;
+    int32_t group_model[3];
+    int32_t group_shared[3];
+    int64_t group_tiles[3];
+    int64_t total_slices;
+    char group_consts[3][1024];
+} tcb_batch_plan;
+
+int64_t tcb_batch_workspace_bytes(int32_t n_sims);
+int tcb_batch_prepare(const tcb_mono* sims, int32_t n_sims, void* workspace, int64_t bytes, tcb_batch_plan* plan);
+/* `steps` batch steps: every listed simulation whose counter is in [1, nt] advances one step each. */
+int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream);
+/* Device error word of the batch (synchronises the stream). */
+int tcb_batch_check(const tcb_batch_plan* plan, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,94 @@
+"""Batched simulations: every result the same alone and in the mix.
+
+Tolerances as in the single-simulation tests: max |dVm| <= 1e-3 * max |Vm_ref|,
+AT/RT within one dt, total CG iterations within 2 %.
+"""
+import numpy as np
+import pytest
+import torch
+
+from tests.golden import cases as C
+from tests.helpers import case_mesh_dir, device_ionic, golden
+
+pytestmark = pytest.mark.gpu
+
+MIX = ["cube6_ms_f32", "cube8_ttp_f32", "ico3_crn_f32", "cube4_ms_period_f32"]
+
+
+def build(case, mesh_dir, device):
+    from torchcor_b200.simulator import Monodomain
+    sim = Monodomain(device_ionic(case, device), T=case["T"], dt=case["dt"], device=device)
+    sim.load_mesh(mesh_dir)
+    for c in case["conductivity"]:
+        sim.add_conductivity(**c)
+    for s in case["stimuli"]:
+        sim.add_stimulus(str(mesh_dir / s["file"]), start=s["start"], duration=s["duration"],
+                         intensity=s["intensity"], period=s.get("period"), count=s.get("count", 1))
+    return sim
+
+
+def outputs(sim):
+    return (sim.activation_time.cpu().numpy(), sim.repolarization_time.cpu().numpy(),
+            sim.solutions.cpu().numpy(), sim.n_total_iter)
+
+
+def assert_close(case, got, ref_at, ref_rt, ref_vm, ref_iters):
+    at, rt, vm, iters = got
+    dt = case["dt"]
+    assert np.abs(at - ref_at).max() <= dt * 1.001
+    assert np.abs(rt - ref_rt).max() <= dt * 1.001
+    assert np.abs(vm - ref_vm).max() <= 1e-3 * np.abs(ref_vm).max()
+    assert abs(iters - ref_iters) <= max(3, ref_iters // 50), (iters, ref_iters)
+
+
+def test_batch_matches_alone_and_reference(lib, cuda, tmp_path):
+    from torchcor_b200.simulator import MonodomainBatch
+    cases = [C.case(n) for n in MIX]
+    dirs = [case_mesh_dir(c, tmp_path) for c in cases]
+    alone = []
+    for c, d in zip(cases, dirs):
+        s = build(c, d, cuda)
+        s.solve(c["tol"], c["tol"], c["max_iter"], verbose=False)
+        alone.append(outputs(s))
+    batch = MonodomainBatch(cuda)
+    sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]) for c, d in zip(cases, dirs)]
+    batch.run()
+    assert not batch.sims
+    for c, s, a in zip(cases, sims, alone):
+        got = outputs(s)
+        assert_close(c, got, *a)
+        g = golden(c["name"])
+        vm = got[2] if "Vm_idx" not in g else got[2][g["Vm_idx"]]
+        assert_close(c, (got[0], got[1], vm, got[3]), g["AT"], g["RT"], g["Vm"], int(g["n_total_iter"]))
+
+
+def test_batch_join_between_steps(lib, cuda, tmp_path):
+    """Simulations that join while others are half way through."""
+    from torchcor_b200.simulator import MonodomainBatch
+    cases = [C.case(n) for n in ("cube8_ttp_f32", "cube6_ms_f32", "ico3_crn_f32")]
+    dirs = [case_mesh_dir(c, tmp_path) for c in cases]
+    batch = MonodomainBatch(cuda)
+    sims = []
+    for k, (c, d) in enumerate(zip(cases, dirs)):
+        sims.append(batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]))
+        batch.step(137 * (k + 1))
+        for s in batch.finished():
+            batch.remove(s)
+    batch.run()
+    for c, s in zip(cases, sims):
+        g = golden(c["name"])
+        got = outputs(s)
+        vm = got[2] if "Vm_idx" not in g else got[2][g["Vm_idx"]]
+        assert_close(c, (got[0], got[1], vm, got[3]), g["AT"], g["RT"], g["Vm"], int(g["n_total_iter"]))
+
+
+def test_batch_of_one_matches_single_path(lib, cuda, tmp_path):
+    from torchcor_b200.simulator import MonodomainBatch
+    c = C.case("cfg1_ms_f32")
+    d = case_mesh_dir(c, tmp_path)
+    single = build(c, d, cuda)
+    single.solve(c["tol"], c["tol"], c["max_iter"], verbose=False)
+    batch = MonodomainBatch(cuda)
+    s = batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"])
+    batch.run()
+    assert_close(c, outputs(s), *outputs(single))

@@ -38,7 +38,8 @@ class tcb_mono(C.Structure):
         ("model", _i32), ("n_states", _i32),
         ("slice_ptr", _vp), ("col", _vp), ("col_delta", _vp), ("m_val", _vp), ("k_val", _vp), ("a_val", _vp), ("d_inv", _vp),
         ("state", _vp), ("tables", _vp),
-        ("x", _vp), ("bprime", _vp), ("r", _vp), ("p", _vp), ("ap", _vp), ("at", _vp), ("rt", _vp),
+        ("x", _vp), ("bprime", _vp), ("r", _vp), ("p", _vp), ("ap", _vp), ("z", _vp), ("p2", _vp),
+        ("at", _vp), ("rt", _vp),
         ("snapshots", _vp),
         ("stim_bits", _vp), ("step_t", _vp), ("step_stim", _vp), ("stim_amp", C.c_float * TCB_MAX_STIMULI),
         ("a_tol", _f64), ("r_tol", _f64),
@@ -46,6 +47,16 @@ class tcb_mono(C.Structure):
         ("cm", C.c_float), ("dt", C.c_float),
         ("step_iters", _vp), ("counter", _vp), ("scratch", _vp), ("barrier", _vp),
         ("params", _vp),
+    ]
+
+
+class tcb_batch_plan(C.Structure):
+    """Mirror of ``struct tcb_batch_plan``."""
+    _fields_ = [
+        ("workspace", _vp),
+        ("n_sims", _i32), ("cg_blocks", _i32), ("cg_smem", _i32), ("n_groups", _i32),
+        ("group_model", _i32 * 3), ("group_shared", _i32 * 3), ("group_tiles", _i64 * 3),
+        ("total_slices", _i64), ("group_consts", (C.c_char * 1024) * 3),
     ]
 
 
@@ -76,6 +87,10 @@ SIGNATURES = [
     ("tcb_mono_run_noalloc", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),
     ("tcb_mono_finish", C.c_int, [C.POINTER(tcb_mono), _vp]),
     ("tcb_mono_check", C.c_int, [C.POINTER(tcb_mono), _vp]),
+    ("tcb_batch_workspace_bytes", _i64, [_i32]),
+    ("tcb_batch_prepare", C.c_int, [C.POINTER(tcb_mono), _i32, _vp, _i64, C.POINTER(tcb_batch_plan)]),
+    ("tcb_batch_run", C.c_int, [C.POINTER(tcb_batch_plan), _i64, _vp]),
+    ("tcb_batch_check", C.c_int, [C.POINTER(tcb_batch_plan), _vp]),
 ]
 
 _lock = threading.Lock()

@@ -25,7 +25,7 @@ LIB = PKG / "libtcb200.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # translation units that must keep float32 expressions as separate roundings
-NO_FMA = {"ionic.cu"}
+NO_FMA = {"ionic.cu", "batch_ionic.cu"}
 
 
 def _nvcc():

@@ -40,11 +40,14 @@ MonoDev make_dev(const tcb_mono* m) {
     d.av = m->a_val;
     d.dinv = m->d_inv;
     d.state = m->state;
+    d.tables = m->tables;
     d.x = m->x;
     d.bp = m->bprime;
     d.r = m->r;
     d.p = m->p;
     d.ap = m->ap;
+    d.z = m->z;
+    d.p2 = m->p2;
     d.at = m->at;
     d.rt = m->rt;
     d.snap = m->snapshots;
@@ -83,6 +86,8 @@ int validate(const tcb_mono* m) {
     return TCB_OK;
 }
 }  // namespace
+
+int validate_mono(const tcb_mono* m) { return validate(m); }
 
 }  // namespace tcb
 

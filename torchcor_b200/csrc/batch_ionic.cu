@@ -1,0 +1,141 @@
+// Batched ionic step: one launch per ionic model covers every simulation of
+// that model in the batch (compiled with -fmad=false, like ionic.cu; the
+// per-node work is the same ionic_node the single-simulation kernel runs).
+//
+// Threads walk a virtual node space made of each simulation's 128-node tiles;
+// a warp's 32 nodes always lie in one tile, so the simulation lookup (binary
+// search over the tile prefix) is warp-uniform.  Model constants are a kernel
+// argument when every simulation of the group shares them (the common case:
+// same parameters and dt), else read per simulation.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include "batch.cuh"
+#include "ionic_crn.cuh"
+#include "ionic_ms.cuh"
+#include "ionic_node.cuh"
+#include "ionic_ttp.cuh"
+#include "tcb_internal.h"
+
+namespace tcb {
+namespace {
+
+constexpr int kThreads = 256;
+
+template <class M, bool SHARED>
+__global__ void __launch_bounds__(kThreads) batch_ionic_kernel(const BatchWS* __restrict__ W, int g,
+                                                               typename M::C c0) {
+    const BatchGroup& G = W->groups[g];
+    const int count = G.count;
+    const int64_t total = G.tile_prefix[count] * kBatchTile;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < total; v += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t tile = v / kBatchTile;
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (G.tile_prefix[mid] <= tile) lo = mid;
+            else hi = mid - 1;
+        }
+        const MonoDev& d = W->dev[G.idx[lo]];
+        const int64_t step = d.counter[0];
+        if (step < 1 || step > d.nt) continue;
+        const int64_t node = (tile - G.tile_prefix[lo]) * kBatchTile + (v % kBatchTile);
+        if (node >= d.n) continue;
+        const typename M::C& c = SHARED ? c0 : static_cast<const typename M::C*>(G.consts)[lo];
+        const typename M::Tables T = static_cast<const typename M::Tables*>(G.tables)[lo];
+        ionic_node<M>(d, c, T, step_view(d, step), node);
+    }
+}
+
+template <class M>
+int launch(const BatchWS* W, int g, int64_t total_tiles, const void* shared_consts, cudaStream_t s) {
+    int64_t blocks = ceil_div(total_tiles * kBatchTile, kThreads);
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks < 1) return TCB_OK;
+    typename M::C c;
+    memset(&c, 0, sizeof c);
+    if (shared_consts) {
+        memcpy(&c, shared_consts, sizeof c);
+        batch_ionic_kernel<M, true><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, c);
+    } else {
+        batch_ionic_kernel<M, false><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, c);
+    }
+    TCB_CHECK_LAUNCH("batched ionic kernel");
+    return TCB_OK;
+}
+
+}  // namespace
+
+size_t model_consts_bytes(int model) {
+    switch (model) {
+        case TCB_MODEL_MS: return sizeof(MS::C);
+        case TCB_MODEL_TTP: return sizeof(TTP::C);
+        case TCB_MODEL_CRN: return sizeof(CRN::C);
+    }
+    return 0;
+}
+
+// Model constant block of a simulation (host), as the kernels read it.
+int model_consts(int model, const double* params, void* out) {
+    switch (model) {
+        case TCB_MODEL_MS: {
+            MS::C c = MS::derive(params);
+            memcpy(out, &c, sizeof c);
+            return TCB_OK;
+        }
+        case TCB_MODEL_TTP: {
+            TTP::C c = TTP::derive(params);
+            memcpy(out, &c, sizeof c);
+            return TCB_OK;
+        }
+        case TCB_MODEL_CRN: {
+            CRN::C c = CRN::derive(params);
+            memcpy(out, &c, sizeof c);
+            return TCB_OK;
+        }
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+size_t model_tables_bytes(int model) {
+    switch (model) {
+        case TCB_MODEL_MS: return sizeof(MS::Tables);
+        case TCB_MODEL_TTP: return sizeof(TTP::Tables);
+        case TCB_MODEL_CRN: return sizeof(CRN::Tables);
+    }
+    return 0;
+}
+
+// Lookup-table view (device pointers into the simulation's table array), host side.
+int model_tables_view(int model, const float* tables, const double* params, void* out) {
+    switch (model) {
+        case TCB_MODEL_MS: {
+            MS::Tables t = MS::tables(tables, params);
+            memcpy(out, &t, sizeof t);
+            return TCB_OK;
+        }
+        case TCB_MODEL_TTP: {
+            TTP::Tables t = TTP::tables(tables, params);
+            memcpy(out, &t, sizeof t);
+            return TCB_OK;
+        }
+        case TCB_MODEL_CRN: {
+            CRN::Tables t = CRN::tables(tables, params);
+            memcpy(out, &t, sizeof t);
+            return TCB_OK;
+        }
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+int launch_batch_ionic(const BatchWS* ws_dev, const BatchWS& host, int g, int64_t total_tiles,
+                       const void* shared_consts, cudaStream_t s) {
+    switch (host.groups[g].model) {
+        case TCB_MODEL_MS: return launch<MS>(ws_dev, g, total_tiles, shared_consts, s);
+        case TCB_MODEL_TTP: return launch<TTP>(ws_dev, g, total_tiles, shared_consts, s);
+        case TCB_MODEL_CRN: return launch<CRN>(ws_dev, g, total_tiles, shared_consts, s);
+    }
+    return fail(TCB_EINVAL, "unknown ionic model in batch");
+}
+
+}  // namespace tcb

@@ -12,6 +12,7 @@
 
 #include "ionic_crn.cuh"
 #include "ionic_ms.cuh"
+#include "ionic_node.cuh"
 #include "ionic_ttp.cuh"
 #include "mono.cuh"
 #include "tcb_internal.h"
@@ -133,58 +134,11 @@ __global__ void differentiate_kernel(typename M::C c, typename M::Tables T, floa
     }
 }
 
-// ------------------------------------------------------------- fused step kernel
-// activation / repolarisation update of monodomain.py:174-176 for time t
-__device__ __forceinline__ void at_rt_update(float u, float t, float* at, float* rt, int64_t i) {
-    float a = at[i];
-    if (u > 0.0f && a == -1.0f) {
-        a = t;
-        at[i] = a;
-    }
-    if (a > 0.0f && u < -70.0f && rt[i] == -1.0f) rt[i] = t;
-}
-
 template <class M>
 __global__ void __launch_bounds__(kThreads) mono_ionic_kernel(MonoDev d, typename M::C c, typename M::Tables T) {
-    const int64_t n = d.counter[0];  // this step (1-based)
-    const float* __restrict__ u = d.x + ring_cur(n) * d.n_pad;
-    const int64_t prev = n - 1;
-    const bool do_atrt = d.at_rt && prev >= 1;
-    const float t_prev = d.step_t[prev];
-    float* snap = (d.snap && d.per_frame > 0 && prev >= 1 && prev % d.per_frame == 0)
-                      ? d.snap + (prev / d.per_frame) * d.n
-                      : nullptr;
-    const uint32_t smask = d.step_stim[n];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float v = u[i];
-        if (do_atrt) at_rt_update(v, t_prev, d.at, d.rt, i);
-        if (snap) snap[i] = v;
-        float s[M::kStates];
-#pragma unroll
-        for (int k = 0; k < M::kStates; ++k) s[k] = d.state[k * d.n_pad + i];
-        const float dV = M::step(v, s, c, T);
-#pragma unroll
-        for (int k = 0; k < M::kStates; ++k) d.state[k * d.n_pad + i] = s[k];
-        // b = u*Cm + dt*du, du = dV/100  (monodomain.py:117-118)
-        float b = v * d.cm + d.dt * (dV / 100.0f);
-        if (smask) {
-            // Istim = sum of the active stimuli in list order (stimulation.py:59-61), /100 (:127)
-            uint32_t bits = d.stim_bits[i] & smask;
-            if (bits) {
-                float I = 0.0f;
-                bool first = true;
-                for (int k = 0; k < TCB_MAX_STIMULI; ++k) {
-                    if ((smask >> k) & 1u) {
-                        float a = ((bits >> k) & 1u) ? d.amp[k] : 0.0f;
-                        I = first ? a : I + a;
-                        first = false;
-                    }
-                }
-                b = b + d.dt * (I / 100.0f);
-            }
-        }
-        d.bp[i] = b;
-    }
+    const StepView sv = step_view(d, d.counter[0]);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += (int64_t)gridDim.x * blockDim.x)
+        ionic_node<M>(d, c, T, sv, i);
 }
 
 __global__ void mono_finish_kernel(MonoDev d) {

@@ -13,7 +13,8 @@ struct MonoDev {
     const int16_t* dcol;   // int16 column offsets from the row, or null
     const float *mv, *kv, *av, *dinv;
     float* state;
-    float *x, *bp, *r, *p, *ap, *at, *rt, *snap;
+    const float* tables;
+    float *x, *bp, *r, *p, *ap, *z, *p2, *at, *rt, *snap;
     const uint32_t* stim_bits;
     const float* step_t;
     const uint32_t* step_stim;

@@ -1,0 +1,91 @@
+"""Many monodomain simulations stepping together on one GPU.
+
+``MonodomainBatch`` holds prepared ``Monodomain`` simulations of any sizes,
+ionic models, time steps and end times.  Every batch step launches one ionic
+kernel per model and one persistent CG kernel for all of them; each simulation
+keeps its own step counter, stimulus schedule, tolerances and iteration count
+(it stops iterating when it converges, the others go on), and simulations can
+join or leave between steps.  Results are the same as running each one alone
+(up to the float64 reduction order inside CG).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from torchcor_b200 import _lib
+from torchcor_b200._lib import check, stream_ptr
+
+MAX_SIMS = 1024
+
+
+class MonodomainBatch:
+    def __init__(self, device=None, max_sims=MAX_SIMS):
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        lib = _lib.load()
+        self.max_sims = max_sims
+        self._ws = torch.empty(int(lib.tcb_batch_workspace_bytes(max_sims)), dtype=torch.uint8, device=self.device)
+        self._plan = _lib.tcb_batch_plan()
+        self._structs = None
+        self.sims = []
+        self._dirty = True
+
+    def add(self, sim, a_tol=1e-5, r_tol=1e-5, max_iter=100, calculate_AT_RT=True, linear_guess=True,
+            snapshot_interval=1):
+        """Prepare ``sim`` (a ``Monodomain`` with mesh, conductivities and stimuli) and add it."""
+        if len(self.sims) >= self.max_sims:
+            raise RuntimeError(f"batch is full ({self.max_sims} simulations)")
+        if sim._sim is None:
+            sim.prepare(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval)
+        self.sims.append(sim)
+        self._dirty = True
+        return sim
+
+    def remove(self, sim, result_path=None):
+        """Take ``sim`` out of the batch; if it has run all its steps, finish it."""
+        self.sims.remove(sim)
+        self._dirty = True
+        if sim._sim["next_step"] > sim.nt:
+            return sim.finish(result_path)
+        return None
+
+    def _prepare(self):
+        n = len(self.sims)
+        arr = (_lib.tcb_mono * n)()
+        for i, s in enumerate(self.sims):
+            arr[i] = s._sim["struct"]
+        self._structs = arr
+        check(_lib.load().tcb_batch_prepare(arr, n, self._ws.data_ptr(), self._ws.numel(), C.byref(self._plan)))
+        self._dirty = False
+
+    def step(self, n_steps=1):
+        """Advance every unfinished simulation by ``n_steps`` steps (asynchronous)."""
+        if not self.sims:
+            return
+        if self._dirty:
+            self._prepare()
+        check(_lib.load().tcb_batch_run(C.byref(self._plan), int(n_steps), stream_ptr()))
+        for s in self.sims:
+            s._sim["next_step"] = min(s._sim["next_step"] + n_steps, s.nt + 1)
+
+    def finished(self):
+        return [s for s in self.sims if s._sim["next_step"] > s.nt]
+
+    def remaining_steps(self):
+        return max((s.nt + 1 - s._sim["next_step"] for s in self.sims), default=0)
+
+    def check(self):
+        if self.sims and not self._dirty:
+            check(_lib.load().tcb_batch_check(C.byref(self._plan), stream_ptr()))
+
+    def run(self, result_paths=None):
+        """Step until every simulation has finished; finish and remove them all."""
+        while self.sims:
+            k = min(s.nt + 1 - s._sim["next_step"] for s in self.sims if s._sim["next_step"] <= s.nt) \
+                if any(s._sim["next_step"] <= s.nt for s in self.sims) else 0
+            if k > 0:
+                self.step(k)
+                self.check()
+            for s in self.finished():
+                self.remove(s, None if result_paths is None else result_paths.get(id(s)))

@@ -109,7 +109,8 @@ class Monodomain:
         t32, mask = self.stimuli.schedule(nt, self.dt)
         sim = dict(
             x=x, bp=torch.zeros(n_pad, **f32), r=torch.zeros(n_pad, **f32), p=torch.zeros(n_pad, **f32),
-            ap=torch.zeros(n_pad, **f32), at=torch.full((n,), -1.0, **f32), rt=torch.full((n,), -1.0, **f32),
+            ap=torch.zeros(n_pad, **f32), z=torch.zeros(n_pad, **f32), p2=torch.zeros(n_pad, **f32),
+            at=torch.full((n,), -1.0, **f32), rt=torch.full((n,), -1.0, **f32),
             snaps=snaps, u0=u0,
             stim_bits=torch.from_numpy(self.stimuli.membership_bits().view(np.int32)).to(dev),
             step_t=torch.from_numpy(t32).to(dev), step_stim=torch.from_numpy(mask.view(np.int32)).to(dev),
@@ -125,7 +126,7 @@ class Monodomain:
         m.slice_ptr, m.col, m.col_delta = ptr(s.slice_ptr), ptr(s.sell_col), ptr(s.sell_dcol)
         m.m_val, m.k_val, m.a_val, m.d_inv = ptr(s.sell_m), ptr(s.sell_k), ptr(s.sell_a), ptr(s.d_inv)
         m.state, m.tables = ptr(im.state), ptr(im.tables)
-        m.x, m.bprime, m.r, m.p, m.ap = (ptr(sim[k]) for k in ("x", "bp", "r", "p", "ap"))
+        m.x, m.bprime, m.r, m.p, m.ap, m.z, m.p2 = (ptr(sim[k]) for k in ("x", "bp", "r", "p", "ap", "z", "p2"))
         m.at, m.rt, m.snapshots = ptr(sim["at"]), ptr(sim["rt"]), ptr(snaps)
         m.stim_bits, m.step_t, m.step_stim = ptr(sim["stim_bits"]), ptr(sim["step_t"]), ptr(sim["step_stim"])
         amp = self.stimuli.amplitudes()
@@ -183,6 +184,35 @@ class Monodomain:
         el = time.time() - t0
         return self.current_solution().clone(), int(sim["step_iters"][n].item()), 0.0, el
 
+    def finish(self, result_path=None, calculate_AT_RT=True):
+        """AT/RT update and snapshot of the last step, error check, result files
+        (the tail of monodomain.py:141-226).  Returns the total CG iterations."""
+        sim = self._sim
+        st = sim["struct"]
+        lib = _lib.load()
+        check(lib.tcb_mono_finish(C.byref(st), stream_ptr()))
+        check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
+        self.n_total_iter = int(sim["step_iters"].sum().item())
+        self.activation_time = sim["at"]
+        self.repolarization_time = sim["rt"]
+        self.solutions = sim["snaps"]
+        if result_path is not None:
+            rp = Path(result_path)
+            rp.mkdir(parents=True, exist_ok=True)
+            if calculate_AT_RT:
+                torch.save(sim["at"].cpu(), rp / "ATs.pt")
+                torch.save(sim["rt"].cpu(), rp / "RTs.pt")
+            if sim["snaps"] is not None:
+                torch.save(sim["snaps"].cpu(), rp / "Vm.pt")
+        return self.n_total_iter
+
+    def prepare(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1):
+        """Assemble and set up the device state of a solve without running it
+        (what ``solve`` does before its loop); used by ``MonodomainBatch``."""
+        self.assemble()
+        return self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval,
+                           snapshot_interval < self.T)
+
     def solve(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1,
               verbose=True, result_path=None):
         self.result_path = Path(result_path) if result_path is not None else None
@@ -200,22 +230,8 @@ class Monodomain:
                 done = sim["next_step"] - 1
                 print(f"t: {round(done * self.dt, 1)}/{self.T}", "Time elapsed:", round(time.time() - t0, 2),
                       flush=True)
-        st = sim["struct"]
-        lib = _lib.load()
-        check(lib.tcb_mono_finish(C.byref(st), stream_ptr()))
-        check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
+        n_total_iter = self.finish(self.result_path if keep or calculate_AT_RT else None, calculate_AT_RT)
         elapsed = time.time() - t0
-        n_total_iter = int(sim["step_iters"].sum().item())
-        self.n_total_iter = n_total_iter
-        self.activation_time = sim["at"]
-        self.repolarization_time = sim["rt"]
-        self.solutions = sim["snaps"]
-        if self.result_path is not None:
-            if calculate_AT_RT:
-                torch.save(sim["at"].cpu(), self.result_path / "ATs.pt")
-                torch.save(sim["rt"].cpu(), self.result_path / "RTs.pt")
-            if keep:
-                torch.save(sim["snaps"].cpu(), self.result_path / "Vm.pt")
         if verbose:
             mem = torch.cuda.max_memory_allocated(self.device) / 1e9
             print(self.ionic_model.name, self.n_nodes, round(elapsed, 2), 0.0, round(elapsed, 2), n_total_iter,
