@@ -306,13 +306,94 @@ def tcb_arm(a, wl, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def batch_arm(a, world, rank, local):
+    """Batched mix (64 cubes, MS/TTP) vs the same simulations one at a time."""
+    from torchcor_b200.simulator import MonodomainBatch
+    from torchcor_b200.workloads import batch_cubes
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    wls = batch_cubes()
+    total = sum(w.n_nodes for w in wls)
+    stream = torch.cuda.current_stream(dev)
+    batch = MonodomainBatch(dev)
+    t0 = time.perf_counter()
+    for w in wls:
+        batch.add(make_sim(w, dev), 1e-5, 1e-5, 100, snapshot_interval=w.T)
+    batch.step(a.warmup)
+    torch.cuda.synchronize(dev)
+    setup_s = time.perf_counter() - t0
+    batch.check()
+    G = a.graph_steps
+    replay = batch.capture(G) if G > 0 else None
+    if replay:
+        replay()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    K = a.steps if not replay else (a.steps // G) * G
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        if replay:
+            for _ in range(K // G):
+                replay()
+        else:
+            batch.step(K)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    batch.check()
+    iters = sum(int(s._sim["step_iters"].sum().item()) for s in batch.sims)
+    # CG passes of the timed steps: the batch kernel runs max_i(it_i + 1) passes a
+    # step; a node needs only its own simulation's it_i + 1
+    lo, hi = a.warmup + 1, a.warmup + K + (G if G else 0)
+    its = torch.stack([s._sim["step_iters"][lo:hi + 1].long() for s in batch.sims])
+    sizes = torch.tensor([s._sim["struct"].n_nodes for s in batch.sims], device=its.device, dtype=torch.float64)
+    passes_max = float((its.max(0).values + 1).double().mean().item())
+    passes_node = float(((its + 1).double() * sizes[:, None]).sum().item() / (sizes.sum().item() * its.shape[1]))
+    value = world * total * K / (ms / 1e3)
+    del batch, replay
+    torch.cuda.empty_cache()
+    # the plain single-simulation path on the same simulations, one after the other
+    plain_ms = 0.0
+    if not a.no_plain:
+        for w in wls:
+            sim = make_sim(w, dev)
+            sim.prepare(1e-5, 1e-5, 100, snapshot_interval=w.T)
+            sim.run_steps(a.warmup)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            sim.run_steps(K)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            plain_ms += e0.elapsed_time(e1)
+            del sim
+    plain = total * K / (plain_ms / 1e3) if plain_ms else None
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": a.warmup,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batch of {len(wls)} tet cubes (16..64 nodes per edge, h 0.25 mm), "
+                                   f"Mitchell-Schaeffer/TTP ENDO 50/50, dt 0.01 ms",
+                       "simulations": len(wls), "nodes": total, "cuda_graph_steps": G,
+                       "cg_iterations_per_step": iters / max(1, (K + a.warmup + (G if G else 0))) / len(wls),
+                       "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,
+                       "setup_s": setup_s},
+            "gpu_launches": 3 * K, "clocks": clk.summary(),
+            "plain_single_path": {"value": plain, "unit": METRIC,
+                                  "what": "each simulation alone through Monodomain (same steps), summed time"},
+            "speedup_vs_plain": (value / plain) if plain else None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="tcb", choices=["tcb", "reference"])
-    ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube"])
+    ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube", "batch_cubes"])
+    ap.add_argument("--graph-steps", type=int, default=0, help="batch mode: steps per captured CUDA graph")
+    ap.add_argument("--no-plain", action="store_true", help="batch mode: skip the one-at-a-time comparison")
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -321,6 +402,11 @@ def main():
         ap.error("--warmup must be at least 3")
     from torchcor_b200.workloads import WORKLOADS
     world, rank, local = dist_setup(a.impl)
+    if a.workload == "batch_cubes":
+        batch_arm(a, world, rank, local)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     wl = WORKLOADS[a.workload]()
     if a.impl == "reference":
         reference_arm(a, wl, world, rank)

@@ -28,6 +28,7 @@ namespace tcb {
 namespace {
 
 using namespace cgk;
+static_assert(sizeof(MonoDev) % 8 == 0, "MonoDev is copied as words and followed by int64 data");
 
 __device__ __forceinline__ float p_update(float z, float p_old, double beta, bool first) {
     return first ? z : (float)(beta * (double)p_old + (double)z);
@@ -39,6 +40,8 @@ __device__ __forceinline__ int col_of(const MonoDev& d, int64_t e, int64_t row) 
 
 struct BatchShared {
     double *rz, *bn, *al, *be, *wp;  // per simulation; wp = [warps][kBatchMaxPerBlock][2]
+    MonoDev* dev;                    // descriptors of the block's simulations
+    int64_t* lsp;                    // their first virtual slice, [kBatchMaxPerBlock + 1]
     int *it, *act, *step;
 };
 
@@ -49,10 +52,21 @@ __device__ __forceinline__ BatchShared carve(double* smd, int n) {
     s.al = s.bn + n;
     s.be = s.al + n;
     s.wp = s.be + n;
-    s.it = reinterpret_cast<int*>(s.wp + kCgWarps * kBatchMaxPerBlock * 2);
+    s.dev = reinterpret_cast<MonoDev*>(s.wp + kCgWarps * kBatchMaxPerBlock * 2);
+    s.lsp = reinterpret_cast<int64_t*>(s.dev + kBatchMaxPerBlock);
+    s.it = reinterpret_cast<int*>(s.lsp + kBatchMaxPerBlock + 1);
     s.act = s.it + n;
     s.step = s.act + n;
     return s;
+}
+
+// copy the descriptors and slice offsets of the block's simulations into shared memory
+__device__ __forceinline__ void stage_descriptors(const BatchWS* W, BatchShared& S, int first, int cnt) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(W->dev + first);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(S.dev);
+    const int words = cnt * (int)(sizeof(MonoDev) / 4);
+    for (int t = threadIdx.x; t < words; t += blockDim.x) dst[t] = src[t];
+    for (int t = threadIdx.x; t <= cnt; t += blockDim.x) S.lsp[t] = W->slice_prefix[first + t];
 }
 
 // warp-reduce two values and add them to this warp's slot of local simulation j
@@ -117,17 +131,19 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
         const int64_t st = W->dev[i].counter[0];
         S.step[i] = (st >= 1 && st <= W->dev[i].nt) ? (int)st : 0;   // 0 = not stepping
     }
+    stage_descriptors(W, S, first, cnt);
     clear_slots(S, cnt);
 
     // ---- right-hand side, guess, r0, z0
     {
-        int i = first;
+        int js = 0;
         for (int64_t vs = vb + warp; vs < ve; vs += kCgWarps) {
-            while (W->slice_prefix[i + 1] <= vs) ++i;
+            while (S.lsp[js + 1] <= vs) ++js;
+            const int i = first + js;
             const int step = S.step[i];
             if (!step) continue;
-            const MonoDev& d = W->dev[i];
-            const int64_t ls = vs - W->slice_prefix[i];
+            const MonoDev& d = S.dev[js];
+            const int64_t ls = vs - S.lsp[js];
             const int64_t row = ls * TCB_SLICE + lane;
             double bb = 0.0, rzl = 0.0;
             if (row < d.n) {
@@ -171,7 +187,7 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
                 bb = db * db;
                 rzl = (double)r32 * (double)z32;
             }
-            warp_add(S, warp, lane, i - first, bb, rzl);
+            warp_add(S, warp, lane, js, bb, rzl);
         }
     }
     publish<2>(W, S, parts0, cnt, off);
@@ -196,15 +212,16 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
         // ---- p = z + beta p (on the fly), Ap, p.Ap
         clear_slots(S, cnt);
         {
-            int i = first;
+            int js = 0;
             for (int64_t vs = vb + warp; vs < ve; vs += kCgWarps) {
-                while (W->slice_prefix[i + 1] <= vs) ++i;
+                while (S.lsp[js + 1] <= vs) ++js;
+                const int i = first + js;
                 if (!S.act[i]) continue;
-                const MonoDev& d = W->dev[i];
+                const MonoDev& d = S.dev[js];
                 const float* pin = (pass & 1) ? d.p2 : d.p;
                 float* pout = (pass & 1) ? d.p : d.p2;
                 const double beta = S.be[i];
-                const int64_t ls = vs - W->slice_prefix[i];
+                const int64_t ls = vs - S.lsp[js];
                 const int64_t row = ls * TCB_SLICE + lane;
                 double pap = 0.0;
                 if (row < d.n) {
@@ -233,7 +250,7 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
                     d.ap[row] = a32;
                     pap = (double)pn * (double)a32;
                 }
-                warp_add(S, warp, lane, i - first, pap, 0.0);
+                warp_add(S, warp, lane, js, pap, 0.0);
             }
         }
         publish<1>(W, S, parts1, cnt, off);
@@ -245,14 +262,15 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
         // ---- x += alpha p, r -= alpha Ap, z = D r; ||z||^2, r.z
         clear_slots(S, cnt);
         {
-            int i = first;
+            int js = 0;
             for (int64_t vs = vb + warp; vs < ve; vs += kCgWarps) {
-                while (W->slice_prefix[i + 1] <= vs) ++i;
+                while (S.lsp[js + 1] <= vs) ++js;
+                const int i = first + js;
                 if (!S.act[i]) continue;
-                const MonoDev& d = W->dev[i];
+                const MonoDev& d = S.dev[js];
                 const float* pnew = (pass & 1) ? d.p : d.p2;
                 const double alpha = S.al[i];
-                const int64_t row = (vs - W->slice_prefix[i]) * TCB_SLICE + lane;
+                const int64_t row = (vs - S.lsp[js]) * TCB_SLICE + lane;
                 double zz = 0.0, rzn = 0.0;
                 if (row < d.n) {
                     float* x = d.x + ring_next(S.step[i]) * d.n_pad;
@@ -264,7 +282,7 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
                     zz = (double)z32 * (double)z32;
                     rzn = (double)r32 * (double)z32;
                 }
-                warp_add(S, warp, lane, i - first, zz, rzn);
+                warp_add(S, warp, lane, js, zz, rzn);
             }
         }
         publish<2>(W, S, parts0, cnt, off);
@@ -295,7 +313,8 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
 }  // namespace
 
 size_t batch_cg_smem(int n) {
-    return (size_t)n * (4 * sizeof(double) + 3 * sizeof(int)) + sizeof(double) * kCgWarps * kBatchMaxPerBlock * 2 + 64;
+    return (size_t)n * (4 * sizeof(double) + 3 * sizeof(int)) + sizeof(double) * kCgWarps * kBatchMaxPerBlock * 2 +
+           sizeof(MonoDev) * kBatchMaxPerBlock + sizeof(int64_t) * (kBatchMaxPerBlock + 1) + 64;
 }
 
 int batch_cg_max_blocks(size_t smem) {

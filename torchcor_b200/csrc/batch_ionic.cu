@@ -20,37 +20,54 @@
 namespace tcb {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = kBatchTile;   // one 128-node tile per block
 
 template <class M, bool SHARED>
 __global__ void __launch_bounds__(kThreads) batch_ionic_kernel(const BatchWS* __restrict__ W, int g,
                                                                typename M::C c0) {
+    __shared__ MonoDev sd;
+    __shared__ typename M::Tables sT;
+    __shared__ int s_lo;
+    __shared__ int64_t s_step;
     const BatchGroup& G = W->groups[g];
-    const int count = G.count;
-    const int64_t total = G.tile_prefix[count] * kBatchTile;
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < total; v += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t tile = v / kBatchTile;
-        int lo = 0, hi = count - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (G.tile_prefix[mid] <= tile) lo = mid;
-            else hi = mid - 1;
+    const int64_t total_tiles = G.tile_prefix[G.count];
+    for (int64_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = G.count - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (G.tile_prefix[mid] <= tile) lo = mid;
+                else hi = mid - 1;
+            }
+            s_lo = lo;
         }
-        const MonoDev& d = W->dev[G.idx[lo]];
-        const int64_t step = d.counter[0];
-        if (step < 1 || step > d.nt) continue;
-        const int64_t node = (tile - G.tile_prefix[lo]) * kBatchTile + (v % kBatchTile);
-        if (node >= d.n) continue;
-        const typename M::C& c = SHARED ? c0 : static_cast<const typename M::C*>(G.consts)[lo];
-        const typename M::Tables T = static_cast<const typename M::Tables*>(G.tables)[lo];
-        ionic_node<M>(d, c, T, step_view(d, step), node);
+        __syncthreads();
+        const int lo = s_lo;
+        {   // stage the simulation's descriptor and table view
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(W->dev + G.idx[lo]);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+            for (int t = threadIdx.x; t < (int)(sizeof(MonoDev) / 4); t += blockDim.x) dst[t] = src[t];
+            const uint32_t* ts = reinterpret_cast<const uint32_t*>(static_cast<const typename M::Tables*>(G.tables) + lo);
+            uint32_t* td = reinterpret_cast<uint32_t*>(&sT);
+            for (int t = threadIdx.x; t < (int)(sizeof(typename M::Tables) / 4); t += blockDim.x) td[t] = ts[t];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_step = sd.counter[0];
+        __syncthreads();
+        const int64_t step = s_step;
+        const int64_t node = (tile - G.tile_prefix[lo]) * kBatchTile + threadIdx.x;
+        if (step >= 1 && step <= sd.nt && node < sd.n) {
+            const typename M::C& c = SHARED ? c0 : static_cast<const typename M::C*>(G.consts)[lo];
+            ionic_node<M>(sd, c, sT, step_view(sd, step), node);
+        }
+        __syncthreads();
     }
 }
 
 template <class M>
 int launch(const BatchWS* W, int g, int64_t total_tiles, const void* shared_consts, cudaStream_t s) {
-    int64_t blocks = ceil_div(total_tiles * kBatchTile, kThreads);
-    if (blocks > 148 * 64) blocks = 148 * 64;
+    int64_t blocks = total_tiles;
+    if (blocks > 148 * 128) blocks = 148 * 128;
     if (blocks < 1) return TCB_OK;
     typename M::C c;
     memset(&c, 0, sizeof c);

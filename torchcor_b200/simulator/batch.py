@@ -69,6 +69,29 @@ class MonodomainBatch:
         for s in self.sims:
             s._sim["next_step"] = min(s._sim["next_step"] + n_steps, s.nt + 1)
 
+    def capture(self, n_steps):
+        """Record ``n_steps`` batch steps in a CUDA graph; returns a callable that
+        replays them (and advances the step bookkeeping).  The batch must not
+        change while the graph is in use; every simulation must have at least
+        ``n_steps`` steps left per replay (finished ones are skipped on the
+        device, the bookkeeping stops at their last step)."""
+        if self._dirty:
+            self._prepare()
+        graph = torch.cuda.CUDAGraph()
+        plan = self._plan
+        lib = _lib.load()
+        with torch.cuda.graph(graph):
+            check(lib.tcb_batch_run(C.byref(plan), int(n_steps), stream_ptr()))
+
+        def replay():
+            if self._dirty:
+                raise RuntimeError("the batch changed after capture; capture again")
+            graph.replay()
+            for s in self.sims:
+                s._sim["next_step"] = min(s._sim["next_step"] + n_steps, s.nt + 1)
+        replay.graph = graph
+        return replay
+
     def finished(self):
         return [s for s in self.sims if s._sim["next_step"] > s.nt]
 

@@ -153,6 +153,24 @@ class Monodomain:
         sim["next_step"] = b
         return b - a
 
+    def capture_steps(self, n_steps):
+        """Record ``n_steps`` steps of the prepared simulation in a CUDA graph;
+        returns a callable replaying them (with the step bookkeeping)."""
+        sim = self._sim
+        lib = _lib.load()
+        # the first launch on a device configures kernel attributes: keep it outside capture
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            check(lib.tcb_mono_run(C.byref(sim["struct"]), 1, 1 + n_steps, stream_ptr()))
+
+        def replay():
+            if sim["next_step"] + n_steps > self.nt + 1:
+                raise RuntimeError("not enough steps left for a full replay")
+            graph.replay()
+            sim["next_step"] += n_steps
+        replay.graph = graph
+        return replay
+
     def current_solution(self):
         sim = self._sim
         return sim["x"][(sim["next_step"] + 2) % 3, : self.n_nodes]

@@ -67,6 +67,32 @@ def ms_cube(n=20, h_mm=1.0, T=50.0, dt=0.01):
                     meta=dict(n=n, h_mm=h_mm))
 
 
+def cube_face_sim(n, h_mm, model, scale, face, T=100.0, dt=0.01, name=None):
+    """One cube of the batched mix: n^3 cells, fibres along +x, conductivity
+    scale * (il=0.5, it=0.2), face ``face`` (0..5 = -x,+x,-y,+y,-z,+z) stimulated
+    at t = 0 for 1 ms with intensity 100."""
+    nodes_um, tets = meshgen.cube(n, h_mm)
+    fib = meshgen.fibres_constant(len(tets))
+    reg = np.ones(len(tets), dtype=np.int64)
+    stims = [dict(region=meshgen.cube_face(n, face // 2, face % 2), start=0.0, duration=1.0, intensity=100)]
+    cond = [dict(region_ids=[1], il=0.5 * scale, it=0.2 * scale)]
+    return Workload(name or f"{model}_cube_{n}", model, nodes_um / 1000.0, tets, reg, fib, cond, stims, dt, T,
+                    meta=dict(n=n, h_mm=h_mm, scale=scale, face=face))
+
+
+def batch_cubes(count=64, seed=2024, lo=16, hi=64, h_mm=0.25, T=100.0, dt=0.01):
+    """``count`` independent cubes: edge length uniform in lo..hi nodes, conductivity
+    scale uniform in [0.5, 2], one random face stimulated, Mitchell-Schaeffer and
+    ten Tusscher-Panfilov ENDO alternating (50/50), dt 0.01 ms, T 100 ms."""
+    rng = np.random.default_rng(seed)
+    edges = rng.integers(lo, hi + 1, size=count)
+    scales = rng.uniform(0.5, 2.0, size=count)
+    faces = rng.integers(0, 6, size=count)
+    return [cube_face_sim(int(e) - 1, h_mm, "ms" if k % 2 == 0 else "ttp", float(sc), int(f), T, dt,
+                          name=f"cube{k}_{int(e)}nodes_{'ms' if k % 2 == 0 else 'ttp'}")
+            for k, (e, sc, f) in enumerate(zip(edges, scales, faces))]
+
+
 WORKLOADS = {"ttp_cube": ttp_cube, "ms_cube": ms_cube}
 
 
