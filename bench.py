@@ -316,6 +316,8 @@ def batch_arm(a, world, rank, local):
     total = sum(w.n_nodes for w in wls)
     stream = torch.cuda.current_stream(dev)
     batch = MonodomainBatch(dev)
+    if a.cg_per_sm:
+        batch.set_cg(a.cg_per_sm)
     t0 = time.perf_counter()
     for w in wls:
         batch.add(make_sim(w, dev), 1e-5, 1e-5, 100, snapshot_interval=w.T)
@@ -323,6 +325,7 @@ def batch_arm(a, world, rank, local):
     torch.cuda.synchronize(dev)
     setup_s = time.perf_counter() - t0
     batch.check()
+    cg_cfg = batch.cg_config
     G = a.graph_steps
     replay = batch.capture(G) if G > 0 else None
     if replay:
@@ -375,6 +378,7 @@ def batch_arm(a, world, rank, local):
             "config": {"workload": f"batch of {len(wls)} tet cubes (16..64 nodes per edge, h 0.25 mm), "
                                    f"Mitchell-Schaeffer/TTP ENDO 50/50, dt 0.01 ms",
                        "simulations": len(wls), "nodes": total, "cuda_graph_steps": G,
+                       "cg_per_sm": cg_cfg[0], "cg_blocks": cg_cfg[1],
                        "cg_iterations_per_step": iters / max(1, (K + a.warmup + (G if G else 0))) / len(wls),
                        "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,
                        "setup_s": setup_s},
@@ -394,6 +398,8 @@ def main():
     ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube", "batch_cubes"])
     ap.add_argument("--graph-steps", type=int, default=0, help="batch mode: steps per captured CUDA graph")
     ap.add_argument("--no-plain", action="store_true", help="batch mode: skip the one-at-a-time comparison")
+    ap.add_argument("--cg-per-sm", type=int, default=0, choices=[0, 1, 2],
+                    help="batch mode: batched CG variant (blocks per SM); 0 = library default")
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

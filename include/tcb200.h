@@ -218,6 +218,7 @@ typedef struct tcb_batch_plan {
     int32_t n_sims, cg_blocks, cg_smem, n_groups;
     int32_t group_model[3];
     int32_t group_shared[3];
+    int32_t cg_per_sm, pad;   /* CG kernel variant: 1 or 2 blocks per SM */
     int64_t group_tiles[3];
     int64_t total_slices;
     char group_consts[3][1024];
@@ -225,6 +226,10 @@ typedef struct tcb_batch_plan {
 
 int64_t tcb_batch_workspace_bytes(int32_t n_sims);
 int tcb_batch_prepare(const tcb_mono* sims, int32_t n_sims, void* workspace, int64_t bytes, tcb_batch_plan* plan);
+/* Switch a prepared plan to the CG kernel variant with `per_sm` (1 or 2) blocks per
+ * SM and the matching grid; TCB_ERANGE if that variant cannot be resident.  No
+ * counterpart in the reference (a tuning knob of this implementation). */
+int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t per_sm);
 /* `steps` batch steps: every listed simulation whose counter is in [1, nt] advances one step each. */
 int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream);
 /* Device error word of the batch (synchronises the stream). */

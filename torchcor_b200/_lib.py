@@ -55,7 +55,8 @@ class tcb_batch_plan(C.Structure):
     _fields_ = [
         ("workspace", _vp),
         ("n_sims", _i32), ("cg_blocks", _i32), ("cg_smem", _i32), ("n_groups", _i32),
-        ("group_model", _i32 * 3), ("group_shared", _i32 * 3), ("group_tiles", _i64 * 3),
+        ("group_model", _i32 * 3), ("group_shared", _i32 * 3), ("cg_per_sm", _i32), ("pad", _i32),
+        ("group_tiles", _i64 * 3),
         ("total_slices", _i64), ("group_consts", (C.c_char * 1024) * 3),
     ]
 
@@ -89,6 +90,7 @@ SIGNATURES = [
     ("tcb_mono_check", C.c_int, [C.POINTER(tcb_mono), _vp]),
     ("tcb_batch_workspace_bytes", _i64, [_i32]),
     ("tcb_batch_prepare", C.c_int, [C.POINTER(tcb_mono), _i32, _vp, _i64, C.POINTER(tcb_batch_plan)]),
+    ("tcb_batch_set_cg", C.c_int, [C.POINTER(tcb_batch_plan), _i32]),
     ("tcb_batch_run", C.c_int, [C.POINTER(tcb_batch_plan), _i64, _vp]),
     ("tcb_batch_check", C.c_int, [C.POINTER(tcb_batch_plan), _vp]),
 ]

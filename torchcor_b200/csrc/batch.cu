@@ -1,6 +1,5 @@
-// Host side of batched simulations: the workspace layout, the plan (block
-// ranges, per-simulation reduction ranges, ionic model groups) and the step
-// loop.
+// Host side of batched simulations: the workspace layout, the plan (CG grid,
+// per-simulation CG views, ionic model groups) and the step loop.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -25,15 +24,25 @@ constexpr size_t kAlign = 256;
 constexpr size_t kMaxConsts = 1024;   // bytes of one model constant block (checked below)
 constexpr size_t kMaxTables = 256;    // bytes of one lookup-table view
 
+constexpr int kDefaultPerSm = 2;      // batched CG blocks per SM unless tuned
+
 size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
+// CG grid for S slices: at least kMinSlicesPerBlock slices a block, at most what is resident
+int cg_grid(int64_t S, size_t smem, int per_sm) {
+    const int cap = batch_cg_max_blocks(smem, per_sm);
+    if (cap < 1) return 0;
+    const int64_t want = ceil_div(S, cgk::kMinSlicesPerBlock);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
+}
+
 struct Layout {
-    size_t ws, dev, slice_prefix, blk_first, blk_count, blk_off, inst_b0, inst_b1, parts, bar, err;
+    size_t ws, dev, cg, slices, parts, bar, err;
     size_t g_idx[kBatchGroups], g_tiles[kBatchGroups], g_consts[kBatchGroups], g_tabs[kBatchGroups];
     size_t total;
 };
 
-Layout layout(int n, int nb) {
+Layout layout(int n) {
     Layout L;
     size_t o = 0;
     auto take = [&](size_t bytes) {
@@ -43,13 +52,9 @@ Layout layout(int n, int nb) {
     };
     L.ws = take(sizeof(BatchWS));
     L.dev = take(sizeof(MonoDev) * n);
-    L.slice_prefix = take(sizeof(int64_t) * (n + 1));
-    L.blk_first = take(sizeof(int32_t) * nb);
-    L.blk_count = take(sizeof(int32_t) * nb);
-    L.blk_off = take(sizeof(int32_t) * nb);
-    L.inst_b0 = take(sizeof(int32_t) * n);
-    L.inst_b1 = take(sizeof(int32_t) * n);
-    L.parts = take(sizeof(double) * 4 * (size_t)(nb + n));
+    L.cg = take(sizeof(CgView) * n);
+    L.slices = take(sizeof(int32_t) * n);
+    L.parts = take(sizeof(double) * 3 * (size_t)n * kBatchMaxBlocks);   // any grid of the plan
     L.bar = take(sizeof(uint32_t) * 4);
     L.err = take(sizeof(int32_t) * 4);
     for (int g = 0; g < kBatchGroups; ++g) {
@@ -69,7 +74,7 @@ using namespace tcb;
 
 extern "C" int64_t tcb_batch_workspace_bytes(int32_t n_sims) {
     if (n_sims < 1 || n_sims > kBatchMaxSims) return -1;
-    return (int64_t)layout(n_sims, cgk::kMaxBlocks).total;
+    return (int64_t)layout(n_sims).total;
 }
 
 extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspace, int64_t bytes,
@@ -81,22 +86,51 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
         if (model_consts_bytes(m) > kMaxConsts || model_tables_bytes(m) > kMaxTables)
             return fail(TCB_EINVAL, "model constants exceed the batch slot");
     std::vector<MonoDev> devs(n);
-    std::vector<int64_t> sp(n + 1, 0);
+    std::vector<CgView> views(n);
+    std::vector<int32_t> slices(n);
+    int64_t S = 0;
     for (int i = 0; i < n; ++i) {
         int st = validate_mono(&sims[i]);
         if (st) return st;
         if (sims[i].n_pad % kBatchTile != 0) return fail(TCB_EINVAL, "n_pad must be a multiple of 128");
         if (!sims[i].z || !sims[i].p2) return fail(TCB_EINVAL, "batched simulations need z and p2 buffers");
+        if (sims[i].n_slices < 1 || sims[i].n_slices > INT32_MAX)
+            return fail(TCB_EINVAL, "simulation slice count out of range");
         devs[i] = make_dev(&sims[i]);
-        sp[i + 1] = sp[i] + sims[i].n_slices;
+        const MonoDev& d = devs[i];
+        CgView& v = views[i];
+        memset(&v, 0, sizeof v);
+        v.n = d.n;
+        v.n_pad = d.n_pad;
+        v.slice_ptr = d.slice_ptr;
+        v.col = d.col;
+        v.dcol = d.dcol;
+        v.mv = d.mv;
+        v.kv = d.kv;
+        v.av = d.av;
+        v.dinv = d.dinv;
+        v.x = d.x;
+        v.bp = d.bp;
+        v.r = d.r;
+        v.p = d.p;
+        v.ap = d.ap;
+        v.z = d.z;
+        v.p2 = d.p2;
+        v.cm = d.cm;
+        v.linear_guess = d.linear_guess;
+        v.a_split = d.a_split;
+        slices[i] = (int32_t)sims[i].n_slices;
+        S += sims[i].n_slices;
     }
-    const int64_t S = sp[n];
     const size_t smem = batch_cg_smem(n);
-    int cap = batch_cg_max_blocks(smem);
-    if (cap < 1) return fail(TCB_ECUDA, "batched CG kernel cannot be resident");
-    int64_t want = ceil_div(S, cgk::kMinSlicesPerBlock);
-    int nb = (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
-    Layout L = layout(n, nb);
+    int per_sm = kDefaultPerSm;
+    int nb = cg_grid(S, smem, per_sm);
+    if (nb < 1) {
+        per_sm = 3 - per_sm;
+        nb = cg_grid(S, smem, per_sm);
+    }
+    if (nb < 1) return fail(TCB_ECUDA, "batched CG kernel cannot be resident");
+    Layout L = layout(n);
     if ((int64_t)L.total > bytes) return fail(TCB_ERANGE, "batch workspace too small");
 
     std::vector<char> host(L.total, 0);
@@ -107,54 +141,16 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
     BatchWS ws;
     memset(&ws, 0, sizeof ws);
     ws.n = n;
-    ws.nb = nb;
-    ws.parts_stride = nb + n;
     ws.total_slices = S;
     ws.dev = reinterpret_cast<const MonoDev*>(dp(L.dev));
-    ws.slice_prefix = reinterpret_cast<const int64_t*>(dp(L.slice_prefix));
-    ws.blk_first = reinterpret_cast<const int32_t*>(dp(L.blk_first));
-    ws.blk_count = reinterpret_cast<const int32_t*>(dp(L.blk_count));
-    ws.blk_off = reinterpret_cast<const int32_t*>(dp(L.blk_off));
-    ws.inst_b0 = reinterpret_cast<const int32_t*>(dp(L.inst_b0));
-    ws.inst_b1 = reinterpret_cast<const int32_t*>(dp(L.inst_b1));
+    ws.cg = reinterpret_cast<const CgView*>(dp(L.cg));
+    ws.slices = reinterpret_cast<const int32_t*>(dp(L.slices));
     ws.parts = reinterpret_cast<double*>(dp(L.parts));
     ws.bar = reinterpret_cast<uint32_t*>(dp(L.bar));
     ws.err = reinterpret_cast<int32_t*>(dp(L.err));
     memcpy(hp(L.dev), devs.data(), sizeof(MonoDev) * n);
-    memcpy(hp(L.slice_prefix), sp.data(), sizeof(int64_t) * (n + 1));
-
-    // block ranges over the virtual slice space and per-simulation block ranges
-    int32_t* bf = reinterpret_cast<int32_t*>(hp(L.blk_first));
-    int32_t* bc = reinterpret_cast<int32_t*>(hp(L.blk_count));
-    int32_t* bo = reinterpret_cast<int32_t*>(hp(L.blk_off));
-    int32_t* b0 = reinterpret_cast<int32_t*>(hp(L.inst_b0));
-    int32_t* b1 = reinterpret_cast<int32_t*>(hp(L.inst_b1));
-    for (int i = 0; i < n; ++i) {
-        b0[i] = nb;
-        b1[i] = -1;
-    }
-    int32_t acc = 0;
-    int i = 0;
-    for (int b = 0; b < nb; ++b) {
-        const int64_t vb = (int64_t)b * S / nb, ve = (int64_t)(b + 1) * S / nb;
-        while (i < n - 1 && sp[i + 1] <= vb) ++i;
-        int last = i;
-        while (last < n - 1 && sp[last + 1] < ve) ++last;
-        if (ve <= vb) last = i - 1;   // empty range (only if S < nb)
-        bf[b] = i;
-        bc[b] = last - i + 1;
-        bo[b] = acc;
-        acc += std::max(0, bc[b]);
-        if (bc[b] > kBatchMaxPerBlock)
-            return fail(TCB_ERANGE, "more than 64 simulations overlap one CG block (too many tiny simulations)");
-        for (int j = i; j <= last; ++j) {
-            b0[j] = std::min(b0[j], b);
-            b1[j] = std::max(b1[j], b);
-        }
-    }
-    if (acc > nb + n) return fail(TCB_EINVAL, "batch partial layout overflow");
-    for (int j = 0; j < n; ++j)
-        if (b1[j] < b0[j]) return fail(TCB_EINVAL, "simulation with no slices in the batch");
+    memcpy(hp(L.cg), views.data(), sizeof(CgView) * n);
+    memcpy(hp(L.slices), slices.data(), sizeof(int32_t) * n);
 
     // ionic groups
     plan->n_groups = 0;
@@ -210,13 +206,27 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
     plan->workspace = workspace;
     plan->n_sims = n;
     plan->cg_blocks = nb;
+    plan->cg_per_sm = per_sm;
+    plan->pad = 0;
     plan->cg_smem = (int32_t)smem;
     plan->total_slices = S;
     return TCB_OK;
 }
 
+extern "C" int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t per_sm) {
+    if (!plan || !plan->workspace || (per_sm != 1 && per_sm != 2))
+        return fail(TCB_EINVAL, "tcb_batch_set_cg: bad arguments");
+    const int nb = cg_grid(plan->total_slices, (size_t)plan->cg_smem, per_sm);
+    if (nb < 1) return fail(TCB_ERANGE, "tcb_batch_set_cg: that CG variant cannot be resident");
+    plan->cg_per_sm = per_sm;
+    plan->cg_blocks = nb;
+    return TCB_OK;
+}
+
 extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream) {
     if (!plan || !plan->workspace || steps < 0) return fail(TCB_EINVAL, "tcb_batch_run: bad arguments");
+    if (plan->cg_blocks < 1 || plan->cg_blocks > kBatchMaxBlocks || (plan->cg_per_sm != 1 && plan->cg_per_sm != 2))
+        return fail(TCB_EINVAL, "tcb_batch_run: plan CG grid out of range");
     cudaStream_t s = as_stream(stream);
     const BatchWS* W = static_cast<const BatchWS*>(plan->workspace);
     BatchWS hv;
@@ -228,7 +238,7 @@ extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* st
                                         plan->group_shared[g] ? plan->group_consts[g] : nullptr, s);
             if (st) return st;
         }
-        int st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, s);
+        int st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_per_sm, s);
         if (st) return st;
     }
     return TCB_OK;

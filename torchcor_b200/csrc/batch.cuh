@@ -1,10 +1,11 @@
 // Device workspace of a batch of monodomain simulations (built by
 // tcb_batch_prepare, read by the batched ionic and CG kernels).
 //
-// The simulations keep their own arrays (MonoDev each).  A virtual slice
-// space (the simulations' 32-row slices one after another) is split evenly
-// over the CG blocks; a virtual tile space (128-node tiles) per ionic model
-// drives the ionic kernels.
+// The simulations keep their own arrays (MonoDev each, plus a compact CgView
+// of the fields the CG kernel reads).  The CG kernel splits the 32-row slices
+// of the simulations that still iterate evenly over its blocks, again at every
+// pass; a virtual tile space (128-node tiles) per ionic model drives the ionic
+// kernels.
 #pragma once
 #include <stdint.h>
 
@@ -13,7 +14,8 @@
 namespace tcb {
 
 constexpr int kBatchMaxSims = 1024;        // simulations per batch
-constexpr int kBatchMaxPerBlock = 64;      // simulations overlapping one CG block's slice range
+constexpr int kBatchMaxPerBlock = 64;      // simulations staged at once by one CG block
+constexpr int kBatchMaxBlocks = 1024;      // CG blocks of a batch
 constexpr int kBatchTile = 128;            // nodes per ionic tile (n_pad is a multiple of it)
 constexpr int kBatchGroups = 3;            // one per ionic model
 
@@ -28,19 +30,25 @@ struct BatchGroup {
     const void* tables;        // [count] lookup-table views (M::Tables)
 };
 
+// what the batched CG kernel reads of one simulation
+struct CgView {
+    int64_t n, n_pad;
+    const int64_t* slice_ptr;
+    const int32_t* col;
+    const int16_t* dcol;       // int16 column offsets from the row, or null
+    const float *mv, *kv, *av, *dinv;
+    float *x, *bp, *r, *p, *ap, *z, *p2;
+    float cm;
+    int32_t linear_guess, a_split, pad;
+};
+
 struct BatchWS {
-    int32_t n, nb;             // simulations, CG blocks
-    int32_t parts_stride;      // nb + n
-    int32_t pad;
+    int32_t n, pad;            // simulations
     int64_t total_slices;
     const MonoDev* dev;        // [n]
-    const int64_t* slice_prefix;  // [n+1]
-    const int32_t* blk_first;  // [nb] first simulation overlapping the block's slice range
-    const int32_t* blk_count;  // [nb] simulations overlapping it
-    const int32_t* blk_off;    // [nb] offset of the block's partials
-    const int32_t* inst_b0;    // [n] first block overlapping the simulation
-    const int32_t* inst_b1;    // [n] last block overlapping it
-    double* parts;             // [2 parities][2 values][parts_stride]
+    const CgView* cg;          // [n]
+    const int32_t* slices;     // [n] 32-row slices of each simulation
+    double* parts;             // [3 values][n][nb] per-simulation block partials
     uint32_t* bar;             // [4] grid barrier words
     int32_t* err;              // [1] error word
     BatchGroup groups[kBatchGroups];
@@ -48,8 +56,8 @@ struct BatchWS {
 
 int launch_batch_ionic(const BatchWS* ws_dev, const BatchWS& ws_host_view, int g, int64_t total_tiles,
                        const void* shared_consts_host, cudaStream_t s);
-int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, cudaStream_t s);
+int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int per_sm, cudaStream_t s);
 size_t batch_cg_smem(int n);
-int batch_cg_max_blocks(size_t smem);
+int batch_cg_max_blocks(size_t smem, int per_sm);   // 0 if that variant cannot be resident
 
 }  // namespace tcb

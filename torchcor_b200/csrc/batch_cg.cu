@@ -3,20 +3,27 @@
 // in one launch, with its own alpha, beta, norms, stopping test and iteration
 // count (per-simulation convergence masks).
 //
-// The simulations' 32-row slices form one virtual slice space split evenly
-// over the blocks.  Vectors live in global memory (a batch is larger than
-// what shared memory holds); the arithmetic is that of the resident
-// single-simulation kernel (fused p-update with a double-buffered p, float64
-// row sums and inner products, int16 column offsets and A rebuilt from M and K'
-// where the simulation allows).
+// Work split.  Simulations converge after different numbers of iterations, so
+// a static split of all slices over the blocks would leave most blocks idle in
+// the late passes while a few carry the simulations that still iterate.
+// Instead, at the start of every pass each block forms the prefix sum of the
+// slice counts of the simulations still active (identical in every block,
+// since every block holds the same scalars) and takes its even share of that
+// virtual slice space.  A pass therefore costs in proportion to the rows still
+// iterating.  Each block's share is contiguous, so neighbouring rows of its
+// simulations stay close in L1/L2.
 //
-// Reductions are per simulation and deterministic: a warp reduces each slice's
-// rows and adds the result to its per-simulation slot in slice order, the
-// block adds its warps' slots in warp order into its partial for each
-// simulation it overlaps, and after the grid barrier every block sums each
-// simulation's partials in block order (a warp per simulation, strided lanes
-// and a fixed shuffle tree), so all blocks hold identical scalars and take
-// identical control-flow decisions.
+// Arithmetic is that of the single-simulation kernels: fused p-update with a
+// double-buffered p, float64 row sums and inner products, int16 column offsets
+// and A rebuilt from M and K' where the simulation allows.
+//
+// Reductions are per simulation and deterministic: each lane accumulates its
+// rows of one simulation in slice order, a warp reduces its lanes with a fixed
+// shuffle tree when its simulation changes, the block adds its warps' values
+// in warp order into its partial slot parts[v][sim][block], and after the grid
+// barrier every block sums each active simulation's partials over the blocks
+// that hold its slices, in block order.  All blocks thus hold identical
+// scalars and take identical control-flow decisions.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -28,267 +35,380 @@ namespace tcb {
 namespace {
 
 using namespace cgk;
-static_assert(sizeof(MonoDev) % 8 == 0, "MonoDev is copied as words and followed by int64 data");
+static_assert(sizeof(CgView) % 8 == 0, "CgView is copied as words");
+static_assert(kBatchMaxSims <= 2 * kCgThreads, "prefix scan covers two simulations per thread");
 
 __device__ __forceinline__ float p_update(float z, float p_old, double beta, bool first) {
     return first ? z : (float)(beta * (double)p_old + (double)z);
 }
 
-__device__ __forceinline__ int col_of(const MonoDev& d, int64_t e, int64_t row) {
-    return d.dcol ? (int)row + (int)__ldg(d.dcol + e) : __ldg(d.col + e);
+// column of ELL entry e of `row`: int16 offset from the row or int32 index
+template <bool DC>
+__device__ __forceinline__ int col_at(const CgView& d, int64_t e, int row) {
+    if constexpr (DC) return row + (int)__ldg(d.dcol + e);
+    else return __ldg(d.col + e);
+}
+
+// Right-hand side, guess, r0 = b - A x0, z0 = D r0 for the 32 rows of slice ls
+// (solver.py:46-55, monodomain.py:130-131); adds ||D b||^2 and r0.z0 into acc.
+// DC: int16 column offsets; AS: A rebuilt as fp32(fp32(M*Cm) + K'); LG: linear
+// extrapolation guess.  Vectors other than x's next slot are read-only here.
+template <bool DC, bool AS, bool LG>
+__device__ __forceinline__ void rhs_slice(const CgView& d, int step, int64_t ls, int lane, double (&acc)[2]) {
+    const int64_t row = ls * TCB_SLICE + lane;
+    if (row >= d.n) return;
+    const float* __restrict__ u = d.x + ring_cur(step) * d.n_pad;
+    const float* __restrict__ xp = d.x + ring_prev(step) * d.n_pad;
+    const float* __restrict__ bp = d.bp;
+    const int64_t s0 = __ldg(d.slice_ptr + ls);
+    const int w = (int)((__ldg(d.slice_ptr + ls + 1) - s0) / TCB_SLICE);
+    const int64_t base = s0 + lane;
+    const int r = (int)row;
+    double mb = 0.0, ku = 0.0, ax = 0.0;
+    for (int k0 = 0; k0 < w; k0 += 4) {
+        int c[4];
+        float mv[4], kv[4], av[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const bool ok = k0 + j < w;
+            const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
+            c[j] = ok ? col_at<DC>(d, e, r) : r;
+            mv[j] = ok ? __ldg(d.mv + e) : 0.0f;
+            kv[j] = ok ? __ldg(d.kv + e) : 0.0f;
+            if constexpr (AS) av[j] = __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]);
+            else av[j] = ok ? __ldg(d.av + e) : 0.0f;
+        }
+        float bc[4], uc[4], xc[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            bc[j] = __ldg(bp + c[j]);
+            uc[j] = __ldg(u + c[j]);
+            if constexpr (LG) xc[j] = __ldg(xp + c[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float xg;
+            if constexpr (LG) xg = 2.0f * uc[j] - xc[j];
+            else xg = uc[j];
+            mb += (double)mv[j] * (double)bc[j];
+            ku += (double)kv[j] * (double)uc[j];
+            ax += (double)av[j] * (double)xg;
+        }
+    }
+    const float rhs = (float)mb - (float)ku;
+    const float ui = __ldg(u + row);
+    float xg0;
+    if constexpr (LG) xg0 = 2.0f * ui - __ldg(xp + row);
+    else xg0 = ui;
+    __stwb(d.x + ring_next(step) * d.n_pad + row, xg0);
+    const float r32 = (float)((double)rhs - ax);
+    const float di = __ldg(d.dinv + row);
+    const float z32 = (float)((double)di * (double)r32);
+    __stwb(d.r + row, r32);
+    __stwb(d.z + row, z32);
+    const double db = (double)di * (double)rhs;
+    acc[0] += db * db;
+    acc[1] += (double)r32 * (double)z32;
+}
+
+// p_new = z + beta p_old formed on the fly for every column, Ap for the rows of
+// slice ls; writes p_new and Ap of its rows and adds p.Ap into acc.  z and p
+// change during the launch, so they are read with plain (L1-allocating)
+// global loads, ordered after their writers by the grid barrier.
+template <bool DC, bool FIRST>
+__device__ __forceinline__ void ap_slice(const CgView& d, const float* pin, float* pout, double beta, int64_t ls,
+                                         int lane, double (&acc)[1]) {
+    const int64_t row = ls * TCB_SLICE + lane;
+    if (row >= d.n) return;
+    const int64_t s0 = __ldg(d.slice_ptr + ls);
+    const int w = (int)((__ldg(d.slice_ptr + ls + 1) - s0) / TCB_SLICE);
+    const int64_t base = s0 + lane;
+    const int r = (int)row;
+    const float* z = d.z;
+    double a = 0.0;
+    for (int k0 = 0; k0 < w; k0 += 8) {
+        int c[8];
+        float av[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const bool ok = k0 + j < w;
+            const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
+            c[j] = ok ? col_at<DC>(d, e, r) : r;
+            av[j] = ok ? __ldg(d.av + e) : 0.0f;
+        }
+        float zc[8], pc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            zc[j] = __ldca(z + c[j]);
+            pc[j] = FIRST ? 0.0f : __ldca(pin + c[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a += (double)av[j] * (double)p_update(zc[j], pc[j], beta, FIRST);
+    }
+    const float pn = p_update(__ldca(z + row), FIRST ? 0.0f : __ldca(pin + row), beta, FIRST);
+    __stwb(pout + row, pn);
+    const float a32 = (float)a;
+    __stwb(d.ap + row, a32);
+    acc[0] += (double)pn * (double)a32;
 }
 
 struct BatchShared {
-    double *rz, *bn, *al, *be, *wp;  // per simulation; wp = [warps][kBatchMaxPerBlock][2]
-    MonoDev* dev;                    // descriptors of the block's simulations
-    int64_t* lsp;                    // their first virtual slice, [kBatchMaxPerBlock + 1]
-    int *it, *act, *step;
+    double *rz, *bn, *al, *be;   // [n] per simulation
+    double* wp;                  // [warps][kBatchMaxPerBlock][2] warp partials of the staged simulations
+    int64_t* pre;                // [n+1] prefix of the active simulations' slice counts
+    int64_t* bb;                 // [nb+1] first virtual slice of each block
+    CgView* cg;                  // [kBatchMaxPerBlock] staged views
+    int *it, *act, *step, *ns;   // [n]
+    int *w0, *w1;                // [n] first and last block holding each active simulation's slices
 };
 
-__device__ __forceinline__ BatchShared carve(double* smd, int n) {
+__device__ __forceinline__ BatchShared carve(double* smd, int n, int nb) {
     BatchShared s;
     s.rz = smd;
     s.bn = s.rz + n;
     s.al = s.bn + n;
     s.be = s.al + n;
     s.wp = s.be + n;
-    s.dev = reinterpret_cast<MonoDev*>(s.wp + kCgWarps * kBatchMaxPerBlock * 2);
-    s.lsp = reinterpret_cast<int64_t*>(s.dev + kBatchMaxPerBlock);
-    s.it = reinterpret_cast<int*>(s.lsp + kBatchMaxPerBlock + 1);
+    s.pre = reinterpret_cast<int64_t*>(s.wp + kCgWarps * kBatchMaxPerBlock * 2);
+    s.bb = s.pre + n + 1;
+    s.cg = reinterpret_cast<CgView*>(s.bb + nb + 1);
+    s.it = reinterpret_cast<int*>(s.cg + kBatchMaxPerBlock);
     s.act = s.it + n;
     s.step = s.act + n;
+    s.ns = s.step + n;
+    s.w0 = s.ns + n;
+    s.w1 = s.w0 + n;
     return s;
 }
 
-// copy the descriptors and slice offsets of the block's simulations into shared memory
-__device__ __forceinline__ void stage_descriptors(const BatchWS* W, BatchShared& S, int first, int cnt) {
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(W->dev + first);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(S.dev);
-    const int words = cnt * (int)(sizeof(MonoDev) / 4);
-    for (int t = threadIdx.x; t < words; t += blockDim.x) dst[t] = src[t];
-    for (int t = threadIdx.x; t <= cnt; t += blockDim.x) S.lsp[t] = W->slice_prefix[first + t];
+// the block whose range [b*A/nb, (b+1)*A/nb) holds virtual slice x
+__device__ __forceinline__ int block_of(int64_t x, int64_t A, int nb) {
+    const int64_t b = ((x + 1) * nb - 1) / A;
+    return b < nb - 1 ? (int)b : nb - 1;
 }
 
-// warp-reduce two values and add them to this warp's slot of local simulation j
-__device__ __forceinline__ void warp_add(BatchShared& S, int warp, int lane, int j, double a, double b) {
-    a = warp_sum(a);
-    b = warp_sum(b);
-    if (lane == 0) {
-        S.wp[(warp * kBatchMaxPerBlock + j) * 2 + 0] += a;
-        S.wp[(warp * kBatchMaxPerBlock + j) * 2 + 1] += b;
+// Exclusive prefix of the slice counts of the simulations with flag[i] != 0
+// into S.pre[0..n], the block boundaries of its even split into S.bb and each
+// simulation's block window into S.w0/S.w1; returns the total.  Every block
+// computes the same.
+__device__ int64_t active_prefix(BatchShared& S, int n, const int* flag) {
+    __shared__ int64_t wt[kCgWarps];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int e0 = 2 * t, e1 = 2 * t + 1;
+    const int64_t v0 = (e0 < n && flag[e0]) ? (int64_t)S.ns[e0] : 0;
+    const int64_t v1 = (e1 < n && flag[e1]) ? (int64_t)S.ns[e1] : 0;
+    int64_t s = v0 + v1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+    }
+    __syncthreads();   // earlier readers of pre and wt are done
+    if (lane == 31) wt[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        int64_t w = lane < kCgWarps ? wt[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kCgWarps) wt[lane] = w;
+    }
+    __syncthreads();
+    const int64_t base = (warp ? wt[warp - 1] : 0) + s - v0 - v1;
+    if (e0 < n) S.pre[e0] = base;
+    if (e1 < n) S.pre[e1] = base + v0;
+    const int64_t total = wt[kCgWarps - 1];
+    if (t == 0) S.pre[n] = total;
+    // the even split of the total over the blocks, and each simulation's blocks
+    const int nb = gridDim.x;
+    for (int b = t; b <= nb; b += blockDim.x) S.bb[b] = (int64_t)b * total / nb;
+    __syncthreads();
+    for (int i = t; i < n; i += blockDim.x) {
+        const int64_t P = S.pre[i], cnt = S.pre[i + 1] - P;
+        S.w0[i] = cnt ? block_of(P, total, nb) : 0;
+        S.w1[i] = cnt ? block_of(P + cnt - 1, total, nb) : -1;
+    }
+    __syncthreads();
+    return total;
+}
+
+// largest i in [0, n) with pre[i] <= x (the active simulation holding virtual slice x)
+__device__ __forceinline__ int sim_of(const int64_t* pre, int n, int64_t x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= x) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+
+// reduce the lanes' NV values and add them to this warp's slot of staged simulation j
+template <int NV>
+__device__ __forceinline__ void flush(BatchShared& S, int warp, int lane, int j, double (&acc)[NV]) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const double t = warp_sum(acc[v]);
+        if (lane == 0) S.wp[(warp * kBatchMaxPerBlock + j) * 2 + v] += t;
+        acc[v] = 0.0;
     }
 }
 
-__device__ __forceinline__ void clear_slots(BatchShared& S, int cnt) {
-    for (int t = threadIdx.x; t < kCgWarps * kBatchMaxPerBlock * 2; t += blockDim.x) S.wp[t] = 0.0;
-    __syncthreads();
-}
-
-// block partials (NV values) of the block's simulations -> parts[value][blk_off + j]
-template <int NV>
-__device__ __forceinline__ void publish(const BatchWS* W, BatchShared& S, double* parts, int cnt, int off) {
-    __syncthreads();
-    for (int j = threadIdx.x; j < cnt; j += blockDim.x)
-        for (int v = 0; v < NV; ++v) {
-            double acc = 0.0;
-            for (int w = 0; w < kCgWarps; ++w) acc += S.wp[(w * kBatchMaxPerBlock + j) * 2 + v];
-            parts[(size_t)v * W->parts_stride + off + j] = acc;
-        }
-}
-
-// every block: totals of every simulation (warp per simulation)
-template <int NV, class F>
-__device__ __forceinline__ void totals(const BatchWS* W, const double* parts, F&& consume) {
+// One sweep over this block's share of the active slices: body(i, view, local
+// slice, acc) adds each lane's row into acc; the block's per-simulation sums go
+// to parts[v][i][block].
+template <int NV, class Body>
+__device__ __forceinline__ void sweep(const BatchWS* W, BatchShared& S, double* parts, Body&& body) {
+    const int nb = gridDim.x, b = blockIdx.x, n = W->n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = warp; i < W->n; i += kCgWarps) {
-        const int b0 = W->inst_b0[i], b1 = W->inst_b1[i];
-        double acc[NV];
-        for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-        for (int b = b0 + lane; b <= b1; b += 32) {
-            const int slot = W->blk_off[b] + (i - W->blk_first[b]);
-            for (int v = 0; v < NV; ++v) acc[v] += __ldcg(parts + (size_t)v * W->parts_stride + slot);
+    const int64_t vb = S.bb[b], ve = S.bb[b + 1];
+    if (vb >= ve) return;
+    const int first = sim_of(S.pre, n, vb), last = sim_of(S.pre, n, ve - 1);
+    for (int j0 = first; j0 <= last; j0 += kBatchMaxPerBlock) {
+        const int j1 = min(last + 1, j0 + kBatchMaxPerBlock);
+        __syncthreads();   // earlier users of the staged views and slots are done
+        {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(W->cg + j0);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(S.cg);
+            const int words = (j1 - j0) * (int)(sizeof(CgView) / 4);
+            for (int t = threadIdx.x; t < words; t += blockDim.x) dst[t] = src[t];
+            for (int t = threadIdx.x; t < kCgWarps * kBatchMaxPerBlock * 2; t += blockDim.x) S.wp[t] = 0.0;
         }
+        __syncthreads();
+        const int64_t sb = max(vb, S.pre[j0]), se = min(ve, S.pre[j1]);
+        double acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+        int i = j0, ci = -1;
+        for (int64_t vs = sb + warp; vs < se; vs += kCgWarps) {
+            while (S.pre[i + 1] <= vs) ++i;
+            if (i != ci) {
+                if (ci >= 0) flush<NV>(S, warp, lane, ci - j0, acc);
+                ci = i;
+            }
+            body(i, S.cg[i - j0], vs - S.pre[i], acc);
+        }
+        if (ci >= 0) flush<NV>(S, warp, lane, ci - j0, acc);
+        __syncthreads();
+        for (int j = threadIdx.x; j < j1 - j0; j += blockDim.x) {
+            const int i2 = j0 + j;
+            if (S.pre[i2 + 1] == S.pre[i2]) continue;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double t = 0.0;
+                for (int w = 0; w < kCgWarps; ++w) t += S.wp[(w * kBatchMaxPerBlock + j) * 2 + v];
+                parts[((size_t)v * n + i2) * nb + b] = t;
+            }
+        }
+    }
+}
+
+// every block: totals of every active simulation (warp per simulation, lanes over its blocks)
+template <int NV, class F>
+__device__ __forceinline__ void totals(const BatchWS* W, BatchShared& S, const double* parts, F&& consume) {
+    const int nb = gridDim.x, n = W->n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = warp; i < n; i += kCgWarps) {
+        const int b0 = S.w0[i], b1 = S.w1[i];
+        if (b1 < b0) continue;   // not active
+        double acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+        for (int bb = b0 + lane; bb <= b1; bb += 32) {
+            if (S.bb[bb] == S.bb[bb + 1]) continue;   // empty block
+#pragma unroll
+            for (int v = 0; v < NV; ++v) acc[v] += __ldcg(parts + ((size_t)v * n + i) * nb + bb);
+        }
+#pragma unroll
         for (int v = 0; v < NV; ++v) acc[v] = warp_sum(acc[v]);
         if (lane == 0) consume(i, acc);
     }
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __restrict__ W) {
+// PER_SM: blocks per SM the register budget is sized for (1: 128 registers a
+// thread, no spills; 2: 64 registers, twice the warps to hide latency)
+template <int PER_SM>
+__global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const BatchWS* __restrict__ W) {
     extern __shared__ double smd[];
-    __shared__ int s_any;
     const int n = W->n;
-    BatchShared S = carve(smd, n);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nb = gridDim.x, b = blockIdx.x;
-    const int64_t vb = (int64_t)b * W->total_slices / nb, ve = (int64_t)(b + 1) * W->total_slices / nb;
-    const int first = W->blk_first[b], cnt = W->blk_count[b], off = W->blk_off[b];
+    BatchShared S = carve(smd, n, gridDim.x);
+    const int lane = threadIdx.x & 31;
     double* parts0 = W->parts;
-    double* parts1 = W->parts + 2 * (size_t)W->parts_stride;
+    double* parts1 = W->parts + 2 * (size_t)n * gridDim.x;
     int32_t* err = W->err;
 
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int64_t st = W->dev[i].counter[0];
         S.step[i] = (st >= 1 && st <= W->dev[i].nt) ? (int)st : 0;   // 0 = not stepping
+        S.ns[i] = W->slices[i];
+        S.act[i] = 0;
+        S.it[i] = 0;
     }
-    stage_descriptors(W, S, first, cnt);
-    clear_slots(S, cnt);
+    __syncthreads();
 
-    // ---- right-hand side, guess, r0, z0
-    {
-        int js = 0;
-        for (int64_t vs = vb + warp; vs < ve; vs += kCgWarps) {
-            while (S.lsp[js + 1] <= vs) ++js;
-            const int i = first + js;
-            const int step = S.step[i];
-            if (!step) continue;
-            const MonoDev& d = S.dev[js];
-            const int64_t ls = vs - S.lsp[js];
-            const int64_t row = ls * TCB_SLICE + lane;
-            double bb = 0.0, rzl = 0.0;
-            if (row < d.n) {
-                const float* u = d.x + ring_cur(step) * d.n_pad;
-                const float* xp = d.x + ring_prev(step) * d.n_pad;
-                float* xn = d.x + ring_next(step) * d.n_pad;
-                const bool lg = d.linear_guess != 0, as = d.a_split != 0;
-                const int64_t base = d.slice_ptr[ls] + lane;
-                const int w = (int)((d.slice_ptr[ls + 1] - d.slice_ptr[ls]) / TCB_SLICE);
-                double mb = 0.0, ku = 0.0, ax = 0.0;
-                for (int k0 = 0; k0 < w; k0 += 4) {
-                    int c[4];
-                    float mv[4], kv[4], av[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const bool ok = k0 + j < w;
-                        const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
-                        c[j] = ok ? col_of(d, e, row) : (int)row;
-                        mv[j] = ok ? __ldg(d.mv + e) : 0.0f;
-                        kv[j] = ok ? __ldg(d.kv + e) : 0.0f;
-                        av[j] = ok ? (as ? __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]) : __ldg(d.av + e)) : 0.0f;
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float uc = u[c[j]];
-                        const float xg = lg ? 2.0f * uc - xp[c[j]] : uc;
-                        mb += (double)mv[j] * (double)d.bp[c[j]];
-                        ku += (double)kv[j] * (double)uc;
-                        ax += (double)av[j] * (double)xg;
-                    }
-                }
-                const float rhs = (float)mb - (float)ku;
-                const float ui = u[row];
-                xn[row] = lg ? 2.0f * ui - xp[row] : ui;
-                const float r32 = (float)((double)rhs - ax);
-                const float di = d.dinv[row];
-                const float z32 = (float)((double)di * (double)r32);
-                d.r[row] = r32;
-                d.z[row] = z32;
-                const double db = (double)di * (double)rhs;
-                bb = db * db;
-                rzl = (double)r32 * (double)z32;
-            }
-            warp_add(S, warp, lane, js, bb, rzl);
+    // ---- right-hand side, guess, r0, z0 (solver.py:46-55; monodomain.py:130-131)
+    int64_t A = active_prefix(S, n, S.step);
+    sweep<2>(W, S, parts0, [&](int i, const CgView& d, int64_t ls, double (&acc)[2]) {
+        const int step = S.step[i];
+        switch ((d.dcol ? 4 : 0) | (d.a_split ? 2 : 0) | (d.linear_guess ? 1 : 0)) {
+            case 0: rhs_slice<false, false, false>(d, step, ls, lane, acc); break;
+            case 1: rhs_slice<false, false, true>(d, step, ls, lane, acc); break;
+            case 2: rhs_slice<false, true, false>(d, step, ls, lane, acc); break;
+            case 3: rhs_slice<false, true, true>(d, step, ls, lane, acc); break;
+            case 4: rhs_slice<true, false, false>(d, step, ls, lane, acc); break;
+            case 5: rhs_slice<true, false, true>(d, step, ls, lane, acc); break;
+            case 6: rhs_slice<true, true, false>(d, step, ls, lane, acc); break;
+            default: rhs_slice<true, true, true>(d, step, ls, lane, acc); break;
         }
-    }
-    publish<2>(W, S, parts0, cnt, off);
+    });
     if (!grid_barrier(W->bar, err)) return;
-    totals<2>(W, parts0, [&](int i, double* t) {
+    totals<2>(W, S, parts0, [&](int i, double* t) {
         S.bn[i] = sqrt(t[0]);
         S.rz[i] = t[1];
         S.be[i] = 0.0;
-        S.it[i] = 0;
-        S.act[i] = S.step[i] != 0 && W->dev[i].max_iter > 0;
+        S.act[i] = W->dev[i].max_iter > 0;
     });
 
     for (int pass = 0;; ++pass) {
-        if (threadIdx.x == 0) {
-            int any = 0;
-            for (int i = 0; i < n; ++i) any |= S.act[i];
-            s_any = any;
-        }
-        __syncthreads();
-        if (!s_any) break;
+        A = active_prefix(S, n, S.act);
+        if (A == 0) break;
         const bool first_pass = pass == 0;
         // ---- p = z + beta p (on the fly), Ap, p.Ap
-        clear_slots(S, cnt);
-        {
-            int js = 0;
-            for (int64_t vs = vb + warp; vs < ve; vs += kCgWarps) {
-                while (S.lsp[js + 1] <= vs) ++js;
-                const int i = first + js;
-                if (!S.act[i]) continue;
-                const MonoDev& d = S.dev[js];
-                const float* pin = (pass & 1) ? d.p2 : d.p;
-                float* pout = (pass & 1) ? d.p : d.p2;
-                const double beta = S.be[i];
-                const int64_t ls = vs - S.lsp[js];
-                const int64_t row = ls * TCB_SLICE + lane;
-                double pap = 0.0;
-                if (row < d.n) {
-                    const int64_t base = d.slice_ptr[ls] + lane;
-                    const int w = (int)((d.slice_ptr[ls + 1] - d.slice_ptr[ls]) / TCB_SLICE);
-                    double a = 0.0;
-                    for (int k0 = 0; k0 < w; k0 += 8) {
-                        int c[8];
-                        float av[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const bool ok = k0 + j < w;
-                            const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
-                            c[j] = ok ? col_of(d, e, row) : (int)row;
-                            av[j] = ok ? __ldg(d.av + e) : 0.0f;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const float pc = first_pass ? 0.0f : pin[c[j]];
-                            a += (double)av[j] * (double)p_update(d.z[c[j]], pc, beta, first_pass);
-                        }
-                    }
-                    const float pn = p_update(d.z[row], first_pass ? 0.0f : pin[row], beta, first_pass);
-                    pout[row] = pn;
-                    const float a32 = (float)a;
-                    d.ap[row] = a32;
-                    pap = (double)pn * (double)a32;
-                }
-                warp_add(S, warp, lane, js, pap, 0.0);
+        sweep<1>(W, S, parts1, [&](int i, const CgView& d, int64_t ls, double (&acc)[1]) {
+            const float* pin = (pass & 1) ? d.p2 : d.p;
+            float* pout = (pass & 1) ? d.p : d.p2;
+            const double beta = S.be[i];
+            if (d.dcol) {
+                if (first_pass) ap_slice<true, true>(d, pin, pout, beta, ls, lane, acc);
+                else ap_slice<true, false>(d, pin, pout, beta, ls, lane, acc);
+            } else {
+                if (first_pass) ap_slice<false, true>(d, pin, pout, beta, ls, lane, acc);
+                else ap_slice<false, false>(d, pin, pout, beta, ls, lane, acc);
             }
-        }
-        publish<1>(W, S, parts1, cnt, off);
-        if (!grid_barrier(W->bar, err)) return;
-        totals<1>(W, parts1, [&](int i, double* t) {
-            if (S.act[i]) S.al[i] = S.rz[i] / t[0];
         });
+        if (!grid_barrier(W->bar, err)) return;
+        totals<1>(W, S, parts1, [&](int i, double* t) { S.al[i] = S.rz[i] / t[0]; });
 
         // ---- x += alpha p, r -= alpha Ap, z = D r; ||z||^2, r.z
-        clear_slots(S, cnt);
-        {
-            int js = 0;
-            for (int64_t vs = vb + warp; vs < ve; vs += kCgWarps) {
-                while (S.lsp[js + 1] <= vs) ++js;
-                const int i = first + js;
-                if (!S.act[i]) continue;
-                const MonoDev& d = S.dev[js];
-                const float* pnew = (pass & 1) ? d.p : d.p2;
-                const double alpha = S.al[i];
-                const int64_t row = (vs - S.lsp[js]) * TCB_SLICE + lane;
-                double zz = 0.0, rzn = 0.0;
-                if (row < d.n) {
-                    float* x = d.x + ring_next(S.step[i]) * d.n_pad;
-                    x[row] = (float)((double)x[row] + alpha * (double)pnew[row]);
-                    const float r32 = (float)((double)d.r[row] - alpha * (double)d.ap[row]);
-                    d.r[row] = r32;
-                    const float z32 = (float)((double)d.dinv[row] * (double)r32);
-                    d.z[row] = z32;
-                    zz = (double)z32 * (double)z32;
-                    rzn = (double)r32 * (double)z32;
-                }
-                warp_add(S, warp, lane, js, zz, rzn);
-            }
-        }
-        publish<2>(W, S, parts0, cnt, off);
+        sweep<2>(W, S, parts0, [&](int i, const CgView& d, int64_t ls, double (&acc)[2]) {
+            const int64_t row = ls * TCB_SLICE + lane;
+            if (row >= d.n) return;
+            const float* pnew = (pass & 1) ? d.p : d.p2;
+            const double alpha = S.al[i];
+            float* x = d.x + ring_next(S.step[i]) * d.n_pad;
+            __stwb(x + row, (float)((double)__ldca(x + row) + alpha * (double)__ldca(pnew + row)));
+            const float r32 = (float)((double)__ldca(d.r + row) - alpha * (double)__ldca(d.ap + row));
+            __stwb(d.r + row, r32);
+            const float z32 = (float)((double)__ldg(d.dinv + row) * (double)r32);
+            __stwb(d.z + row, z32);
+            acc[0] += (double)z32 * (double)z32;
+            acc[1] += (double)r32 * (double)z32;
+        });
         if (!grid_barrier(W->bar, err)) return;
-        totals<2>(W, parts0, [&](int i, double* t) {
-            if (!S.act[i]) return;
+        totals<2>(W, S, parts0, [&](int i, double* t) {
             const MonoDev& d = W->dev[i];
             const double zn = sqrt(t[0]);
             if (zn < d.a_tol || (zn / S.bn[i]) < d.r_tol) {   // solver.py:66-69
@@ -301,10 +421,11 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
             if (S.it[i] >= d.max_iter) S.act[i] = 0;
         });
     }
-    // each simulation's first block records its iterations and advances its step
-    if (threadIdx.x == 0)
-        for (int i = first; i < first + cnt; ++i)
-            if (W->inst_b0[i] == b && S.step[i]) {
+    // block 0 records the iterations and advances the step counters (every
+    // block read the counters before the first grid barrier)
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            if (S.step[i]) {
                 W->dev[i].step_iters[S.step[i]] = S.it[i];
                 W->dev[i].counter[0] = S.step[i] + 1;
             }
@@ -313,21 +434,33 @@ __global__ void __launch_bounds__(kCgThreads) batch_cg_kernel(const BatchWS* __r
 }  // namespace
 
 size_t batch_cg_smem(int n) {
-    return (size_t)n * (4 * sizeof(double) + 3 * sizeof(int)) + sizeof(double) * kCgWarps * kBatchMaxPerBlock * 2 +
-           sizeof(MonoDev) * kBatchMaxPerBlock + sizeof(int64_t) * (kBatchMaxPerBlock + 1) + 64;
+    return (size_t)n * (4 * sizeof(double) + 6 * sizeof(int)) + sizeof(double) * kCgWarps * kBatchMaxPerBlock * 2 +
+           sizeof(int64_t) * (n + 1) + sizeof(int64_t) * (kBatchMaxBlocks + 1) + sizeof(CgView) * kBatchMaxPerBlock +
+           64;
 }
 
-int batch_cg_max_blocks(size_t smem) {
+template <int PER_SM>
+int max_blocks(size_t smem) {
     int dev = 0, sms = 0, occ = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(batch_cg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_cg_kernel, kCgThreads, smem);
-    int cap = sms * occ;
-    return cap > kMaxBlocks ? kMaxBlocks : cap;
+    if (cudaFuncSetAttribute(batch_cg_kernel<PER_SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_cg_kernel<PER_SM>, kCgThreads, smem) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (occ > PER_SM) occ = PER_SM;
+    const int cap = sms * occ;
+    return cap > kBatchMaxBlocks ? kBatchMaxBlocks : cap;
 }
 
-int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, cudaStream_t s) {
+int batch_cg_max_blocks(size_t smem, int per_sm) {
+    return per_sm == 1 ? max_blocks<1>(smem) : per_sm == 2 ? max_blocks<2>(smem) : 0;
+}
+
+int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int per_sm, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nb);
     cfg.blockDim = dim3(kCgThreads);
@@ -338,7 +471,10 @@ int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, cudaStream_t s) 
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel, ws_dev));
+    if (per_sm == 1)
+        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<1>, ws_dev));
+    else
+        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<2>, ws_dev));
     return TCB_OK;
 }
 

@@ -30,6 +30,7 @@ class MonodomainBatch:
         self._structs = None
         self.sims = []
         self._dirty = True
+        self._cg_per_sm = None
 
     def add(self, sim, a_tol=1e-5, r_tol=1e-5, max_iter=100, calculate_AT_RT=True, linear_guess=True,
             snapshot_interval=1):
@@ -56,8 +57,26 @@ class MonodomainBatch:
         for i, s in enumerate(self.sims):
             arr[i] = s._sim["struct"]
         self._structs = arr
-        check(_lib.load().tcb_batch_prepare(arr, n, self._ws.data_ptr(), self._ws.numel(), C.byref(self._plan)))
+        lib = _lib.load()
+        check(lib.tcb_batch_prepare(arr, n, self._ws.data_ptr(), self._ws.numel(), C.byref(self._plan)))
+        if self._cg_per_sm is not None:
+            check(lib.tcb_batch_set_cg(C.byref(self._plan), int(self._cg_per_sm)))
         self._dirty = False
+
+    def set_cg(self, per_sm):
+        """Use the batched CG kernel variant sized for ``per_sm`` (1 or 2) blocks per SM."""
+        if per_sm not in (1, 2):
+            raise ValueError("per_sm must be 1 or 2")
+        self._cg_per_sm = per_sm
+        if self.sims and not self._dirty:
+            check(_lib.load().tcb_batch_set_cg(C.byref(self._plan), int(per_sm)))
+
+    @property
+    def cg_config(self):
+        """(blocks per SM, CG blocks) of the current plan."""
+        if self._dirty and self.sims:
+            self._prepare()
+        return int(self._plan.cg_per_sm), int(self._plan.cg_blocks)
 
     def step(self, n_steps=1):
         """Advance every unfinished simulation by ``n_steps`` steps (asynchronous)."""
