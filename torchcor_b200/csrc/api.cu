@@ -77,6 +77,7 @@ int validate(const tcb_mono* m) {
     if (m->n_nodes <= 0 || m->n_pad < m->n_nodes || m->n_pad % 128 != 0 ||
         m->n_slices != ceil_div(m->n_nodes, TCB_SLICE) || m->nt < 0)
         return fail(TCB_EINVAL, "tcb_mono: inconsistent sizes");
+    if (m->nt >= INT32_MAX) return fail(TCB_ERANGE, "tcb_mono: more than 2^31 - 2 time steps");
     if (!m->slice_ptr || !m->col || !m->m_val || !m->k_val || !m->a_val || !m->d_inv || !m->state || !m->x ||
         !m->bprime || !m->r || !m->p || !m->ap || !m->at || !m->rt || !m->stim_bits || !m->step_t ||
         !m->step_stim || !m->step_iters || !m->counter || !m->scratch || !m->barrier || !m->params)

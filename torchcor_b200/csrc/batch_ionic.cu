@@ -3,8 +3,8 @@
 // per-node work is the same ionic_node the single-simulation kernel runs).
 //
 // Threads walk a virtual node space made of each simulation's 128-node tiles;
-// a warp's 32 nodes always lie in one tile, so the simulation lookup (binary
-// search over the tile prefix) is warp-uniform.  Model constants are a kernel
+// a tile always lies in one simulation, so the simulation lookup (binary search
+// over the tile prefix) is block-uniform.  Model constants are a kernel
 // argument when every simulation of the group shares them (the common case:
 // same parameters and dt), else read per simulation.
 #include <cuda_runtime.h>
@@ -20,55 +20,69 @@
 namespace tcb {
 namespace {
 
-constexpr int kThreads = kBatchTile;   // one 128-node tile per block
+constexpr int kThreads = kBatchTile;   // a block walks 128-node tiles
+constexpr int kTilesPerBlock = 8;      // consecutive tiles per block
 
+// resident blocks per SM the register budget is sized for (MS: 42 registers)
+template <class M>
+constexpr int min_blocks() { return M::kStates > 4 ? 8 : 12; }
+
+// A block covers tiles [blockIdx.x * 8, +8) of the group's virtual tile space;
+// consecutive tiles mostly belong to one simulation, so its descriptor, table
+// view and step view are set up once and again only when the walk crosses into
+// the next simulation (the only points where the block syncs).
 template <class M, bool SHARED>
-__global__ void __launch_bounds__(kThreads) batch_ionic_kernel(const BatchWS* __restrict__ W, int g,
-                                                               typename M::C c0) {
+__global__ void __launch_bounds__(kThreads, min_blocks<M>()) batch_ionic_kernel(const BatchWS* __restrict__ W,
+                                                                                int g, typename M::C c0) {
     __shared__ MonoDev sd;
     __shared__ typename M::Tables sT;
     __shared__ int s_lo;
-    __shared__ int64_t s_step;
     const BatchGroup& G = W->groups[g];
     const int64_t total_tiles = G.tile_prefix[G.count];
-    for (int64_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-        if (threadIdx.x == 0) {
-            int lo = 0, hi = G.count - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (G.tile_prefix[mid] <= tile) lo = mid;
-                else hi = mid - 1;
+    const int64_t t0 = (int64_t)blockIdx.x * kTilesPerBlock;
+    const int64_t t1 = t0 + kTilesPerBlock < total_tiles ? t0 + kTilesPerBlock : total_tiles;
+    int lo = -1;
+    int64_t first = 0, next = 0, step = 0;
+    StepView sv = {};
+    for (int64_t tile = t0; tile < t1; ++tile) {
+        if (tile >= next) {   // block-uniform: entering a new simulation
+            if (lo >= 0) __syncthreads();   // every thread is done with the staged view
+            if (threadIdx.x == 0) {
+                int l = lo < 0 ? 0 : lo + 1, h = G.count - 1;
+                while (l < h) {
+                    const int mid = (l + h + 1) >> 1;
+                    if (G.tile_prefix[mid] <= tile) l = mid;
+                    else h = mid - 1;
+                }
+                s_lo = l;
             }
-            s_lo = lo;
-        }
-        __syncthreads();
-        const int lo = s_lo;
-        {   // stage the simulation's descriptor and table view
+            __syncthreads();
+            lo = s_lo;
             const uint32_t* src = reinterpret_cast<const uint32_t*>(W->dev + G.idx[lo]);
             uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
             for (int t = threadIdx.x; t < (int)(sizeof(MonoDev) / 4); t += blockDim.x) dst[t] = src[t];
             const uint32_t* ts = reinterpret_cast<const uint32_t*>(static_cast<const typename M::Tables*>(G.tables) + lo);
             uint32_t* td = reinterpret_cast<uint32_t*>(&sT);
             for (int t = threadIdx.x; t < (int)(sizeof(typename M::Tables) / 4); t += blockDim.x) td[t] = ts[t];
+            first = G.tile_prefix[lo];
+            next = G.tile_prefix[lo + 1];
+            __syncthreads();
+            step = sd.counter[0];
+            if (step >= 1 && step <= sd.nt) sv = step_view(sd, step);
         }
-        __syncthreads();
-        if (threadIdx.x == 0) s_step = sd.counter[0];
-        __syncthreads();
-        const int64_t step = s_step;
-        const int64_t node = (tile - G.tile_prefix[lo]) * kBatchTile + threadIdx.x;
+        const int64_t node = (tile - first) * kBatchTile + threadIdx.x;
         if (step >= 1 && step <= sd.nt && node < sd.n) {
             const typename M::C& c = SHARED ? c0 : static_cast<const typename M::C*>(G.consts)[lo];
-            ionic_node<M>(sd, c, sT, step_view(sd, step), node);
+            ionic_node<M>(sd, c, sT, sv, node);
         }
-        __syncthreads();
     }
 }
 
 template <class M>
 int launch(const BatchWS* W, int g, int64_t total_tiles, const void* shared_consts, cudaStream_t s) {
-    int64_t blocks = total_tiles;
-    if (blocks > 148 * 128) blocks = 148 * 128;
+    const int64_t blocks = (total_tiles + kTilesPerBlock - 1) / kTilesPerBlock;
     if (blocks < 1) return TCB_OK;
+    if (blocks > INT32_MAX) return fail(TCB_ERANGE, "batched ionic grid too large");
     typename M::C c;
     memset(&c, 0, sizeof c);
     if (shared_consts) {

@@ -31,8 +31,9 @@ __device__ __forceinline__ StepView step_view(const MonoDev& d, int64_t n) {
     const int64_t prev = n - 1;
     v.do_atrt = d.at_rt && prev >= 1;
     v.t_prev = d.step_t[prev];
-    v.snap = (d.snap && d.per_frame > 0 && prev >= 1 && prev % d.per_frame == 0) ? d.snap + (prev / d.per_frame) * d.n
-                                                                                 : nullptr;
+    // step numbers and frame intervals are below 2^31 (validated on the host)
+    const uint32_t pv = (uint32_t)prev, pf = (uint32_t)d.per_frame;
+    v.snap = (d.snap && d.per_frame > 0 && prev >= 1 && pv % pf == 0u) ? d.snap + (int64_t)(pv / pf) * d.n : nullptr;
     v.smask = d.step_stim[n];
     return v;
 }
