@@ -65,34 +65,40 @@ __device__ __forceinline__ void rhs_slice(const CgView& d, int step, int64_t ls,
     const int64_t base = s0 + lane;
     const int r = (int)row;
     double mb = 0.0, ku = 0.0, ax = 0.0;
+    // the columns of the next 4-entry chunk are loaded while this chunk's
+    // gathers and coefficients are in flight (a column load heads each chain)
+    int c[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) c[j] = j < w ? col_at<DC>(d, base + (int64_t)j * TCB_SLICE, r) : r;
     for (int k0 = 0; k0 < w; k0 += 4) {
-        int c[4];
-        float mv[4], kv[4], av[4];
+        float mv[4], kv[4], av[4], bc[4], uc[4], xc[4];
+        int cn[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const bool ok = k0 + j < w;
             const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
-            c[j] = ok ? col_at<DC>(d, e, r) : r;
             mv[j] = ok ? __ldg(d.mv + e) : 0.0f;
             kv[j] = ok ? __ldg(d.kv + e) : 0.0f;
-            if constexpr (AS) av[j] = __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]);
-            else av[j] = ok ? __ldg(d.av + e) : 0.0f;
-        }
-        float bc[4], uc[4], xc[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
+            if constexpr (!AS) av[j] = ok ? __ldg(d.av + e) : 0.0f;
             bc[j] = __ldg(bp + c[j]);
             uc[j] = __ldg(u + c[j]);
             if constexpr (LG) xc[j] = __ldg(xp + c[j]);
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
+            const bool ok = k0 + 4 + j < w;
+            cn[j] = ok ? col_at<DC>(d, base + (int64_t)(k0 + 4 + j) * TCB_SLICE, r) : r;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if constexpr (AS) av[j] = __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]);
             float xg;
             if constexpr (LG) xg = 2.0f * uc[j] - xc[j];
             else xg = uc[j];
             mb += (double)mv[j] * (double)bc[j];
             ku += (double)kv[j] * (double)uc[j];
             ax += (double)av[j] * (double)xg;
+            c[j] = cn[j];
         }
     }
     const float rhs = (float)mb - (float)ku;
