@@ -325,6 +325,11 @@ def batch_arm(a, world, rank, local):
     torch.cuda.synchronize(dev)
     setup_s = time.perf_counter() - t0
     batch.check()
+    tuned = None
+    if not a.cg_per_sm:
+        from torchcor_b200.tune import tune_batch
+        tuned = tune_batch(batch, steps=10)[1]
+        torch.cuda.synchronize(dev)
     cg_cfg = batch.cg_config
     G = a.graph_steps
     replay = batch.capture(G) if G > 0 else None
@@ -379,6 +384,7 @@ def batch_arm(a, world, rank, local):
                                    f"Mitchell-Schaeffer/TTP ENDO 50/50, dt 0.01 ms",
                        "simulations": len(wls), "nodes": total, "cuda_graph_steps": G,
                        "cg_per_sm": cg_cfg[0], "cg_blocks": cg_cfg[1],
+                       "autotune_ms_per_step": tuned,
                        "cg_iterations_per_step": iters / max(1, (K + a.warmup + (G if G else 0))) / len(wls),
                        "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,
                        "setup_s": setup_s},
@@ -389,13 +395,39 @@ def batch_arm(a, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def serving_arm(a, world, rank, local):
+    """Request stream served on one GPU per rank (independent replicas); prints
+    throughput and p50/p99 request latency."""
+    from torchcor_b200 import serving
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    reqs = serving.generate_requests(count=a.requests, seed=2025 + rank, capacity=a.capacity, load=a.load)
+    server = serving.Server(dev)
+    with ClockSampler(local) as clk:
+        summ = server.run(reqs)
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": summ["node_steps_per_s"] * world, "unit": METRIC, "n_gpus": world,
+            "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"serving: {a.requests} requests, Poisson arrivals offered at {a.load} x "
+                                   f"{a.capacity:.3g} node-steps/s, N lognormal(median 50k) in [10k, 500k], "
+                                   f"cube/icosphere 50/50, MS/TTP/CRN, T U(50,300) ms, dt 0.01 ms",
+                       "parallelism": "replicas only"},
+            "serving": summ, "gpu_launches": None, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="tcb", choices=["tcb", "reference"])
-    ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube", "batch_cubes"])
+    ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube", "batch_cubes", "serving"])
+    ap.add_argument("--requests", type=int, default=512, help="serving mode: requests in the stream")
+    ap.add_argument("--load", type=float, default=0.9, help="serving mode: offered load / capacity")
+    ap.add_argument("--capacity", type=float, default=5e9, help="serving mode: node-steps/s the rate assumes")
     ap.add_argument("--graph-steps", type=int, default=0, help="batch mode: steps per captured CUDA graph")
     ap.add_argument("--no-plain", action="store_true", help="batch mode: skip the one-at-a-time comparison")
     ap.add_argument("--cg-per-sm", type=int, default=0, choices=[0, 1, 2],
@@ -408,6 +440,11 @@ def main():
         ap.error("--warmup must be at least 3")
     from torchcor_b200.workloads import WORKLOADS
     world, rank, local = dist_setup(a.impl)
+    if a.workload == "serving":
+        serving_arm(a, world, rank, local)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if a.workload == "batch_cubes":
         batch_arm(a, world, rank, local)
         if world > 1:

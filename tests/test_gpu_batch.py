@@ -92,3 +92,27 @@ def test_batch_of_one_matches_single_path(lib, cuda, tmp_path):
     s = batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"])
     batch.run()
     assert_close(c, outputs(s), *outputs(single))
+
+
+def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
+    """The tuner times real steps of the batch with each CG variant, keeps the
+    fastest, caches it, and the simulations still match the reference."""
+    from torchcor_b200.simulator import MonodomainBatch
+    from torchcor_b200.tune import CG_VARIANTS, TuneCache, tune_batch
+    cases = [C.case(n) for n in ("cube6_ms_f32", "cube8_ttp_f32")]
+    dirs = [case_mesh_dir(c, tmp_path) for c in cases]
+    cache = TuneCache(tmp_path / "tune.json")
+    batch = MonodomainBatch(cuda)
+    sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]) for c, d in zip(cases, dirs)]
+    choice, times = tune_batch(batch, steps=3, cache=cache)
+    assert choice in CG_VARIANTS and set(times) == set(CG_VARIANTS)
+    assert batch.cg_config[0] == choice
+    assert len(cache.load()) == 1
+    again, t2 = tune_batch(batch, steps=3, cache=cache)
+    assert again == choice and t2 is None          # served from the cache
+    batch.run()
+    for c, s in zip(cases, sims):
+        g = golden(c["name"])
+        got = outputs(s)
+        vm = got[2] if "Vm_idx" not in g else got[2][g["Vm_idx"]]
+        assert_close(c, (got[0], got[1], vm, got[3]), g["AT"], g["RT"], g["Vm"], int(g["n_total_iter"]))

@@ -111,6 +111,31 @@ def icosphere(level: int, radius_mm: float):
     return nodes, np.asarray(faces, dtype=np.int64)
 
 
+def icosphere_fast(level: int, radius_mm: float):
+    """``icosphere`` with the subdivision vectorised (same faces and node order:
+    new midpoint nodes are numbered in order of their edge's first appearance)."""
+    nodes0, faces0 = icosphere(0, 1.0)
+    verts = nodes0 / 1000.0
+    faces = faces0
+    for _ in range(level):
+        a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
+        e = np.stack([np.stack([a, b], 1), np.stack([b, c], 1), np.stack([c, a], 1)], 1).reshape(-1, 2)
+        key = np.minimum(e[:, 0], e[:, 1]) * (len(verts) + 1) + np.maximum(e[:, 0], e[:, 1])
+        uniq, first, inv = np.unique(key, return_index=True, return_inverse=True)
+        order = np.argsort(first, kind="stable")
+        rank = np.empty_like(order)
+        rank[order] = np.arange(len(order))
+        ue = e[first[order]]
+        m = verts[ue[:, 0]] + verts[ue[:, 1]]
+        m /= np.sqrt((m * m).sum(1))[:, None]
+        mid_id = (len(verts) + rank[inv]).reshape(-1, 3)
+        ab, bc, ca = mid_id[:, 0], mid_id[:, 1], mid_id[:, 2]
+        faces = np.stack([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1), np.stack([c, ca, bc], 1),
+                          np.stack([ab, bc, ca], 1)], 1).reshape(-1, 3)
+        verts = np.concatenate([verts, m])
+    return verts * (radius_mm * 1000.0), faces.astype(np.int64)
+
+
 def fibres_random_tangent(nodes_um, tris, seed: int):
     """Unit fibre per triangle, uniform angle in the plane normal to the centroid."""
     c = centroids(nodes_um, tris)

@@ -71,6 +71,15 @@ class MonodomainBatch:
         if self.sims and not self._dirty:
             check(_lib.load().tcb_batch_set_cg(C.byref(self._plan), int(per_sm)))
 
+    def autotune(self, steps=10, cache=None, force=False):
+        """Choose the batched CG variant for this batch's shape on this GPU
+        (cached; on a miss it times real steps of the batch, see
+        ``torchcor_b200.tune.tune_batch``).  Returns the blocks-per-SM choice."""
+        from torchcor_b200.tune import tune_batch
+        if self._dirty and self.sims:
+            self._prepare()
+        return tune_batch(self, steps=steps, cache=cache, force=force)[0]
+
     @property
     def cg_config(self):
         """(blocks per SM, CG blocks) of the current plan."""
