@@ -21,26 +21,29 @@ namespace tcb {
 namespace {
 
 constexpr int kThreads = kBatchTile;   // a block walks 128-node tiles
-constexpr int kTilesPerBlock = 8;      // consecutive tiles per block
+constexpr int kMaxTilesPerBlock = 8;   // consecutive tiles per block, at most
+constexpr int kBlocksPerSmTarget = 16; // fewer tiles per block when the group is small
 
 // resident blocks per SM the register budget is sized for (MS: 42 registers)
 template <class M>
 constexpr int min_blocks() { return M::kStates > 4 ? 8 : 12; }
 
-// A block covers tiles [blockIdx.x * 8, +8) of the group's virtual tile space;
+// A block covers tiles [blockIdx.x * tpb, +tpb) of the group's virtual tile
+// space (tpb = 1..8, so that small groups still fill the GPU);
 // consecutive tiles mostly belong to one simulation, so its descriptor, table
 // view and step view are set up once and again only when the walk crosses into
 // the next simulation (the only points where the block syncs).
 template <class M, bool SHARED>
 __global__ void __launch_bounds__(kThreads, min_blocks<M>()) batch_ionic_kernel(const BatchWS* __restrict__ W,
-                                                                                int g, typename M::C c0) {
+                                                                                int g, int tpb,
+                                                                                typename M::C c0) {
     __shared__ MonoDev sd;
     __shared__ typename M::Tables sT;
     __shared__ int s_lo;
     const BatchGroup& G = W->groups[g];
     const int64_t total_tiles = G.tile_prefix[G.count];
-    const int64_t t0 = (int64_t)blockIdx.x * kTilesPerBlock;
-    const int64_t t1 = t0 + kTilesPerBlock < total_tiles ? t0 + kTilesPerBlock : total_tiles;
+    const int64_t t0 = (int64_t)blockIdx.x * tpb;
+    const int64_t t1 = t0 + tpb < total_tiles ? t0 + tpb : total_tiles;
     int lo = -1;
     int64_t first = 0, next = 0, step = 0;
     StepView sv = {};
@@ -80,16 +83,21 @@ __global__ void __launch_bounds__(kThreads, min_blocks<M>()) batch_ionic_kernel(
 
 template <class M>
 int launch(const BatchWS* W, int g, int64_t total_tiles, const void* shared_consts, cudaStream_t s) {
-    const int64_t blocks = (total_tiles + kTilesPerBlock - 1) / kTilesPerBlock;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t per_block = (total_tiles + (int64_t)sms * kBlocksPerSmTarget - 1) / ((int64_t)sms * kBlocksPerSmTarget);
+    const int tpb = (int)(per_block < 1 ? 1 : per_block > kMaxTilesPerBlock ? kMaxTilesPerBlock : per_block);
+    const int64_t blocks = (total_tiles + tpb - 1) / tpb;
     if (blocks < 1) return TCB_OK;
     if (blocks > INT32_MAX) return fail(TCB_ERANGE, "batched ionic grid too large");
     typename M::C c;
     memset(&c, 0, sizeof c);
     if (shared_consts) {
         memcpy(&c, shared_consts, sizeof c);
-        batch_ionic_kernel<M, true><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, c);
+        batch_ionic_kernel<M, true><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, tpb, c);
     } else {
-        batch_ionic_kernel<M, false><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, c);
+        batch_ionic_kernel<M, false><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, tpb, c);
     }
     TCB_CHECK_LAUNCH("batched ionic kernel");
     return TCB_OK;
