@@ -316,8 +316,8 @@ def batch_arm(a, world, rank, local):
     total = sum(w.n_nodes for w in wls)
     stream = torch.cuda.current_stream(dev)
     batch = MonodomainBatch(dev)
-    if a.cg_per_sm:
-        batch.set_cg(a.cg_per_sm)
+    if a.cg_variant:
+        batch.set_cg(a.cg_variant)
     t0 = time.perf_counter()
     for w in wls:
         batch.add(make_sim(w, dev), 1e-5, 1e-5, 100, snapshot_interval=w.T)
@@ -326,7 +326,7 @@ def batch_arm(a, world, rank, local):
     setup_s = time.perf_counter() - t0
     batch.check()
     tuned = None
-    if not a.cg_per_sm:
+    if not a.cg_variant:
         from torchcor_b200.tune import tune_batch
         tuned = tune_batch(batch, steps=10)[1]
         torch.cuda.synchronize(dev)
@@ -383,7 +383,7 @@ def batch_arm(a, world, rank, local):
             "config": {"workload": f"batch of {len(wls)} tet cubes (16..64 nodes per edge, h 0.25 mm), "
                                    f"Mitchell-Schaeffer/TTP ENDO 50/50, dt 0.01 ms",
                        "simulations": len(wls), "nodes": total, "cuda_graph_steps": G,
-                       "cg_per_sm": cg_cfg[0], "cg_blocks": cg_cfg[1],
+                       "cg_variant": cg_cfg[0], "cg_blocks": cg_cfg[1],
                        "autotune_ms_per_step": tuned,
                        "cg_iterations_per_step": iters / max(1, (K + a.warmup + (G if G else 0))) / len(wls),
                        "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,
@@ -430,8 +430,8 @@ def main():
     ap.add_argument("--capacity", type=float, default=5e9, help="serving mode: node-steps/s the rate assumes")
     ap.add_argument("--graph-steps", type=int, default=0, help="batch mode: steps per captured CUDA graph")
     ap.add_argument("--no-plain", action="store_true", help="batch mode: skip the one-at-a-time comparison")
-    ap.add_argument("--cg-per-sm", type=int, default=0, choices=[0, 1, 2],
-                    help="batch mode: batched CG variant (blocks per SM); 0 = library default")
+    ap.add_argument("--cg-variant", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="batch mode: batched CG variant (1/2 streaming, 3 staged); 0 = autotuned")
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

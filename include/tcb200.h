@@ -218,7 +218,11 @@ typedef struct tcb_batch_plan {
     int32_t n_sims, cg_blocks, cg_smem, n_groups;
     int32_t group_model[3];
     int32_t group_shared[3];
-    int32_t cg_per_sm, pad;   /* CG kernel variant: 1 or 2 blocks per SM */
+    int32_t cg_variant;       /* CG kernel: 1 / 2 = streaming sized for 1 / 2 blocks per SM,
+                                 3 = ELL streams staged in shared memory by bulk copies */
+    int32_t cg_stage_bytes;   /* staging bytes per warp and stage (variant 3) */
+    int32_t cg_stage_ok;      /* 1 if every ELL array allows bulk copies (16-byte aligned) */
+    int32_t pad;
     int64_t group_tiles[3];
     int64_t total_slices;
     char group_consts[3][1024];
@@ -226,10 +230,11 @@ typedef struct tcb_batch_plan {
 
 int64_t tcb_batch_workspace_bytes(int32_t n_sims);
 int tcb_batch_prepare(const tcb_mono* sims, int32_t n_sims, void* workspace, int64_t bytes, tcb_batch_plan* plan);
-/* Switch a prepared plan to the CG kernel variant with `per_sm` (1 or 2) blocks per
- * SM and the matching grid; TCB_ERANGE if that variant cannot be resident.  No
- * counterpart in the reference (a tuning knob of this implementation). */
-int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t per_sm);
+/* Switch a prepared plan to CG kernel variant 1, 2 or 3 (see cg_variant) and the
+ * matching grid; TCB_ERANGE if that variant cannot be resident or (3) the arrays
+ * do not allow bulk copies.  No counterpart in the reference (a tuning knob of
+ * this implementation). */
+int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant);
 /* `steps` batch steps: every listed simulation whose counter is in [1, nt] advances one step each. */
 int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream);
 /* Device error word of the batch (synchronises the stream). */

@@ -41,7 +41,10 @@ def assert_close(case, got, ref_at, ref_rt, ref_vm, ref_iters):
     assert abs(iters - ref_iters) <= max(3, ref_iters // 50), (iters, ref_iters)
 
 
-def test_batch_matches_alone_and_reference(lib, cuda, tmp_path):
+@pytest.mark.parametrize("variant", [2, 1, 3])
+def test_batch_matches_alone_and_reference(lib, cuda, tmp_path, variant):
+    """Every batched CG variant (streaming for 2 or 1 blocks per SM, and the one
+    staging the ELL streams in shared memory by bulk copies)."""
     from torchcor_b200.simulator import MonodomainBatch
     cases = [C.case(n) for n in MIX]
     dirs = [case_mesh_dir(c, tmp_path) for c in cases]
@@ -52,6 +55,9 @@ def test_batch_matches_alone_and_reference(lib, cuda, tmp_path):
         alone.append(outputs(s))
     batch = MonodomainBatch(cuda)
     sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]) for c, d in zip(cases, dirs)]
+    assert variant in batch.cg_variants()
+    batch.set_cg(variant)
+    assert batch.cg_config[0] == variant
     batch.run()
     assert not batch.sims
     for c, s, a in zip(cases, sims, alone):
@@ -105,7 +111,7 @@ def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
     batch = MonodomainBatch(cuda)
     sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]) for c, d in zip(cases, dirs)]
     choice, times = tune_batch(batch, steps=3, cache=cache)
-    assert choice in CG_VARIANTS and set(times) == set(CG_VARIANTS)
+    assert choice in CG_VARIANTS and set(times) == set(batch.cg_variants())
     assert batch.cg_config[0] == choice
     assert len(cache.load()) == 1
     again, t2 = tune_batch(batch, steps=3, cache=cache)

@@ -7,10 +7,10 @@ from torchcor_b200 import tune
 def test_cache_roundtrip(tmp_path):
     c = tune.TuneCache(tmp_path / "sub" / "tune.json")
     assert c.get("k") is None
-    c.put("k", {"cg_per_sm": 2})
-    c.put("k2", {"cg_per_sm": 1})
-    assert c.get("k") == {"cg_per_sm": 2}
-    assert json.loads((tmp_path / "sub" / "tune.json").read_text())["k2"] == {"cg_per_sm": 1}
+    c.put("k", {"cg_variant": 2})
+    c.put("k2", {"cg_variant": 1})
+    assert c.get("k") == {"cg_variant": 2}
+    assert json.loads((tmp_path / "sub" / "tune.json").read_text())["k2"] == {"cg_variant": 1}
 
 
 def test_cache_survives_garbage(tmp_path):
@@ -18,8 +18,8 @@ def test_cache_survives_garbage(tmp_path):
     p.write_text("{not json")
     c = tune.TuneCache(p)
     assert c.get("x") is None
-    c.put("x", {"cg_per_sm": 1})
-    assert c.get("x") == {"cg_per_sm": 1}
+    c.put("x", {"cg_variant": 1})
+    assert c.get("x") == {"cg_variant": 1}
 
 
 def test_cache_path_env(tmp_path, monkeypatch):

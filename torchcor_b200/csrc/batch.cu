@@ -24,13 +24,13 @@ constexpr size_t kAlign = 256;
 constexpr size_t kMaxConsts = 1024;   // bytes of one model constant block (checked below)
 constexpr size_t kMaxTables = 256;    // bytes of one lookup-table view
 
-constexpr int kDefaultPerSm = 2;      // batched CG blocks per SM unless tuned
+constexpr int kDefaultVariant = 2;    // batched CG variant unless tuned
 
 size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 // CG grid for S slices: at least kMinSlicesPerBlock slices a block, at most what is resident
-int cg_grid(int64_t S, size_t smem, int per_sm) {
-    const int cap = batch_cg_max_blocks(smem, per_sm);
+int cg_grid(int64_t S, size_t smem, int variant) {
+    const int cap = batch_cg_max_blocks(smem, variant);
     if (cap < 1) return 0;
     const int64_t want = ceil_div(S, cgk::kMinSlicesPerBlock);
     return (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
@@ -122,14 +122,23 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
         slices[i] = (int32_t)sims[i].n_slices;
         S += sims[i].n_slices;
     }
-    const size_t smem = batch_cg_smem(n);
-    int per_sm = kDefaultPerSm;
-    int nb = cg_grid(S, smem, per_sm);
+    int variant = kDefaultVariant;
+    size_t smem = batch_cg_smem_variant(n, variant);
+    int nb = cg_grid(S, smem, variant);
     if (nb < 1) {
-        per_sm = 3 - per_sm;
-        nb = cg_grid(S, smem, per_sm);
+        variant = 1;
+        smem = batch_cg_smem_variant(n, variant);
+        nb = cg_grid(S, smem, variant);
     }
     if (nb < 1) return fail(TCB_ECUDA, "batched CG kernel cannot be resident");
+    // bulk copies need 16-byte aligned sources (slices start at multiples of 32 entries)
+    int stage_ok = batch_cg_stage_bytes(n) > 0;
+    for (int i = 0; i < n && stage_ok; ++i) {
+        const CgView& v = views[i];
+        const void* ptrs[5] = {v.dcol ? (const void*)v.dcol : (const void*)v.col, v.mv, v.kv, v.av, nullptr};
+        for (int k = 0; k < 4; ++k)
+            if (reinterpret_cast<uintptr_t>(ptrs[k]) % 16 != 0) stage_ok = 0;
+    }
     Layout L = layout(n);
     if ((int64_t)L.total > bytes) return fail(TCB_ERANGE, "batch workspace too small");
 
@@ -206,26 +215,34 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
     plan->workspace = workspace;
     plan->n_sims = n;
     plan->cg_blocks = nb;
-    plan->cg_per_sm = per_sm;
+    plan->cg_variant = variant;
+    plan->cg_stage_bytes = 0;
+    plan->cg_stage_ok = stage_ok;
     plan->pad = 0;
     plan->cg_smem = (int32_t)smem;
     plan->total_slices = S;
     return TCB_OK;
 }
 
-extern "C" int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t per_sm) {
-    if (!plan || !plan->workspace || (per_sm != 1 && per_sm != 2))
+extern "C" int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant) {
+    if (!plan || !plan->workspace || variant < 1 || variant > 3)
         return fail(TCB_EINVAL, "tcb_batch_set_cg: bad arguments");
-    const int nb = cg_grid(plan->total_slices, (size_t)plan->cg_smem, per_sm);
+    if (variant == 3 && !plan->cg_stage_ok)
+        return fail(TCB_ERANGE, "tcb_batch_set_cg: staged CG needs 16-byte aligned ELL arrays and shared memory");
+    const size_t smem = batch_cg_smem_variant(plan->n_sims, variant);
+    const int nb = cg_grid(plan->total_slices, smem, variant);
     if (nb < 1) return fail(TCB_ERANGE, "tcb_batch_set_cg: that CG variant cannot be resident");
-    plan->cg_per_sm = per_sm;
+    plan->cg_variant = variant;
+    plan->cg_stage_bytes = variant == 3 ? batch_cg_stage_bytes(plan->n_sims) : 0;
+    plan->cg_smem = (int32_t)smem;
     plan->cg_blocks = nb;
     return TCB_OK;
 }
 
 extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream) {
     if (!plan || !plan->workspace || steps < 0) return fail(TCB_EINVAL, "tcb_batch_run: bad arguments");
-    if (plan->cg_blocks < 1 || plan->cg_blocks > kBatchMaxBlocks || (plan->cg_per_sm != 1 && plan->cg_per_sm != 2))
+    if (plan->cg_blocks < 1 || plan->cg_blocks > kBatchMaxBlocks || plan->cg_variant < 1 || plan->cg_variant > 3 ||
+        (plan->cg_variant == 3 && (!plan->cg_stage_ok || plan->cg_stage_bytes < 2048)))
         return fail(TCB_EINVAL, "tcb_batch_run: plan CG grid out of range");
     cudaStream_t s = as_stream(stream);
     const BatchWS* W = static_cast<const BatchWS*>(plan->workspace);
@@ -238,7 +255,7 @@ extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* st
                                         plan->group_shared[g] ? plan->group_consts[g] : nullptr, s);
             if (st) return st;
         }
-        int st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_per_sm, s);
+        int st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_variant, plan->cg_stage_bytes, s);
         if (st) return st;
     }
     return TCB_OK;

@@ -56,8 +56,12 @@ struct BatchWS {
 
 int launch_batch_ionic(const BatchWS* ws_dev, const BatchWS& ws_host_view, int g, int64_t total_tiles,
                        const void* shared_consts_host, cudaStream_t s);
-int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int per_sm, cudaStream_t s);
+// batched CG variants: 1 / 2 = streaming, sized for 1 / 2 blocks per SM;
+// 3 = ELL streams staged in shared memory by bulk copies, 1 block per SM
+int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int stage_bytes, cudaStream_t s);
 size_t batch_cg_smem(int n);
-int batch_cg_max_blocks(size_t smem, int per_sm);   // 0 if that variant cannot be resident
+size_t batch_cg_smem_variant(int n, int variant);
+int batch_cg_stage_bytes(int n);                    // 0 if the staged variant does not fit
+int batch_cg_max_blocks(size_t smem, int variant);  // 0 if that variant cannot be resident
 
 }  // namespace tcb

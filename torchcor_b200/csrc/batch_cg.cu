@@ -38,8 +38,10 @@ using namespace cgk;
 static_assert(sizeof(CgView) % 8 == 0, "CgView is copied as words");
 static_assert(kBatchMaxSims <= 2 * kCgThreads, "prefix scan covers two simulations per thread");
 
-__device__ __forceinline__ float p_update(float z, float p_old, double beta, bool first) {
-    return first ? z : (float)(beta * (double)p_old + (double)z);
+// p_new = z + beta p_old in float32 (one rounding, a fused multiply-add with
+// beta rounded to float32); every row that forms a given p_new gets the same value
+__device__ __forceinline__ float p_update(float z, float p_old, float beta, bool first) {
+    return first ? z : __fmaf_rn(beta, p_old, z);
 }
 
 // column of ELL entry e of `row`: int16 offset from the row or int32 index
@@ -64,7 +66,10 @@ __device__ __forceinline__ void rhs_slice(const CgView& d, int step, int64_t ls,
     const int w = (int)((__ldg(d.slice_ptr + ls + 1) - s0) / TCB_SLICE);
     const int64_t base = s0 + lane;
     const int r = (int)row;
-    double mb = 0.0, ku = 0.0, ax = 0.0;
+    // M b' and K u accumulate in float32 (the reference's float32 products),
+    // A x0 in float64 (the reference's CG is float64; b - A x0 cancels)
+    float mb = 0.0f, ku = 0.0f;
+    double ax = 0.0;
     // the columns of the next 4-entry chunk are loaded while this chunk's
     // gathers and coefficients are in flight (a column load heads each chain)
     int c[4];
@@ -95,13 +100,13 @@ __device__ __forceinline__ void rhs_slice(const CgView& d, int step, int64_t ls,
             float xg;
             if constexpr (LG) xg = 2.0f * uc[j] - xc[j];
             else xg = uc[j];
-            mb += (double)mv[j] * (double)bc[j];
-            ku += (double)kv[j] * (double)uc[j];
+            mb = __fmaf_rn(mv[j], bc[j], mb);
+            ku = __fmaf_rn(kv[j], uc[j], ku);
             ax += (double)av[j] * (double)xg;
             c[j] = cn[j];
         }
     }
-    const float rhs = (float)mb - (float)ku;
+    const float rhs = mb - ku;
     const float ui = __ldg(u + row);
     float xg0;
     if constexpr (LG) xg0 = 2.0f * ui - __ldg(xp + row);
@@ -122,7 +127,7 @@ __device__ __forceinline__ void rhs_slice(const CgView& d, int step, int64_t ls,
 // change during the launch, so they are read with plain (L1-allocating)
 // global loads, ordered after their writers by the grid barrier.
 template <bool DC, bool FIRST>
-__device__ __forceinline__ void ap_slice(const CgView& d, const float* pin, float* pout, double beta, int64_t ls,
+__device__ __forceinline__ void ap_slice(const CgView& d, const float* pin, float* pout, float beta, int64_t ls,
                                          int lane, double (&acc)[1]) {
     const int64_t row = ls * TCB_SLICE + lane;
     if (row >= d.n) return;
@@ -157,6 +162,103 @@ __device__ __forceinline__ void ap_slice(const CgView& d, const float* pin, floa
     __stwb(d.ap + row, a32);
     acc[0] += (double)pn * (double)a32;
 }
+
+// ---------------------------------------------------------------------------
+// Staged variant: the sliced-ELL streams (columns and coefficients) of the next
+// units are copied into shared memory by bulk asynchronous copies
+// (cp.async.bulk, completion counted on an mbarrier) while the warp works on
+// the current unit, so only the gathers of neighbour values are exposed to
+// memory latency.  A unit is up to 16 entries of one 32-row slice: in every
+// ELL array its entries are one contiguous block (column-major slices).
+constexpr int kStages = 2;             // units in flight per warp
+constexpr int kMaxUnitEntries = 16;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// global -> shared bulk copy (no multicast); 16-byte aligned addresses, size a multiple of 16
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// warp-uniform wait for a stage's copies; gives up after the barrier timeout
+// (error word set) so a lost copy can never hang the kernel
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* err) {
+    if (__all_sync(0xffffffffu, mbar_test(bar, parity))) return true;
+    const uint64_t t0 = globaltimer();
+    while (!__all_sync(0xffffffffu, mbar_test(bar, parity))) {
+        if (globaltimer() - t0 > kBarrierTimeoutNs) {
+            if ((threadIdx.x & 31) == 0) atomicCAS(err, 0, TCB_ETIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+
+struct Pipe {
+    unsigned char* buf;   // this warp's kStages buffers of stage_bytes
+    uint64_t* bar;        // their mbarriers
+    uint32_t phase;       // bit s: parity of stage s's next completion
+    int stage_bytes;
+};
+
+struct Row {
+    double v[3];   // per-row partial sums carried across a slice's units
+};
+
+// what a phase streams: columns, then its coefficient arrays
+struct RhsStreams {
+    __device__ static int entry_bytes(const CgView& d) { return (d.dcol ? 2 : 4) + 8 + (d.a_split ? 0 : 4); }
+    __device__ static void copy(const CgView& d, int64_t e0, int nk, unsigned char* dst, uint64_t* bar) {
+        const uint32_t m = (uint32_t)nk * TCB_SLICE;
+        if (d.dcol) {
+            bulk_load(dst, d.dcol + e0, m * 2, bar);
+            dst += m * 2;
+        } else {
+            bulk_load(dst, d.col + e0, m * 4, bar);
+            dst += m * 4;
+        }
+        bulk_load(dst, d.mv + e0, m * 4, bar);
+        bulk_load(dst + m * 4, d.kv + e0, m * 4, bar);
+        if (!d.a_split) bulk_load(dst + m * 8, d.av + e0, m * 4, bar);
+    }
+};
+
+struct ApStreams {
+    __device__ static int entry_bytes(const CgView& d) { return (d.dcol ? 2 : 4) + 4; }
+    __device__ static void copy(const CgView& d, int64_t e0, int nk, unsigned char* dst, uint64_t* bar) {
+        const uint32_t m = (uint32_t)nk * TCB_SLICE;
+        if (d.dcol) {
+            bulk_load(dst, d.dcol + e0, m * 2, bar);
+            dst += m * 2;
+        } else {
+            bulk_load(dst, d.col + e0, m * 4, bar);
+            dst += m * 4;
+        }
+        bulk_load(dst, d.av + e0, m * 4, bar);
+    }
+};
 
 struct BatchShared {
     double *rz, *bn, *al, *be;   // [n] per simulation
@@ -311,6 +413,247 @@ __device__ __forceinline__ void sweep(const BatchWS* W, BatchShared& S, double* 
     }
 }
 
+// A warp's walk over the units of its slices vs = start, start+16, ... < se
+// (all values warp-uniform).
+template <class Streams>
+struct Walk {
+    int64_t vs, se, ls, s0;
+    int i, w, k0, nk;
+    bool ok;
+    __device__ void load(const BatchShared& S, int j0, int stage_bytes) {
+        ok = vs < se;
+        if (!ok) return;
+        while (S.pre[i + 1] <= vs) ++i;
+        const CgView& d = S.cg[i - j0];
+        ls = vs - S.pre[i];
+        s0 = __ldg(d.slice_ptr + ls);
+        w = (int)((__ldg(d.slice_ptr + ls + 1) - s0) / TCB_SLICE);
+        const int fit = stage_bytes / (TCB_SLICE * Streams::entry_bytes(d));
+        nk = fit < kMaxUnitEntries ? fit : kMaxUnitEntries;
+        k0 = 0;
+    }
+    __device__ void next(const BatchShared& S, int j0, int stage_bytes) {
+        k0 += nk;
+        if (k0 >= w) {
+            vs += kCgWarps;
+            load(S, j0, stage_bytes);
+        }
+    }
+    __device__ int count() const { return nk < w - k0 ? nk : w - k0; }
+};
+
+template <class Streams>
+__device__ __forceinline__ void issue(Pipe& P, int s, const CgView& d, const Walk<Streams>& u, int lane) {
+    if (lane == 0) {
+        const int nk = u.count();
+        // order this warp's earlier shared-memory reads of the stage before the async writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_tx(P.bar + s, (uint32_t)(nk * TCB_SLICE * Streams::entry_bytes(d)));
+        Streams::copy(d, u.s0 + (int64_t)u.k0 * TCB_SLICE, nk, P.buf + (size_t)s * P.stage_bytes, P.bar + s);
+    }
+}
+
+// sweep() with the ELL streams staged: unit(i, view, ls, nk, stage buffer, row)
+// accumulates one unit into the row's partial sums, end(i, view, ls, row, acc)
+// finishes a row after its slice's last unit.  Returns false after a timed-out
+// wait (the error word is set; the caller's next grid barrier ends the kernel).
+template <int NV, class Streams, class Unit, class End>
+__device__ __forceinline__ bool sweep_staged(const BatchWS* W, BatchShared& S, double* parts, Pipe& P,
+                                             int32_t* err, Unit&& unit, End&& end) {
+    const int nb = gridDim.x, b = blockIdx.x, n = W->n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t vb = S.bb[b], ve = S.bb[b + 1];
+    if (vb >= ve) return true;
+    bool good = true;
+    const int first = sim_of(S.pre, n, vb), last = sim_of(S.pre, n, ve - 1);
+    for (int j0 = first; j0 <= last; j0 += kBatchMaxPerBlock) {
+        const int j1 = min(last + 1, j0 + kBatchMaxPerBlock);
+        __syncthreads();   // earlier users of the staged views and slots are done
+        {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(W->cg + j0);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(S.cg);
+            const int words = (j1 - j0) * (int)(sizeof(CgView) / 4);
+            for (int t = threadIdx.x; t < words; t += blockDim.x) dst[t] = src[t];
+            for (int t = threadIdx.x; t < kCgWarps * kBatchMaxPerBlock * 2; t += blockDim.x) S.wp[t] = 0.0;
+        }
+        __syncthreads();
+        Walk<Streams> cons;
+        cons.vs = max(vb, S.pre[j0]) + warp;
+        cons.se = min(ve, S.pre[j1]);
+        cons.i = j0;
+        cons.load(S, j0, P.stage_bytes);
+        Walk<Streams> prod = cons;
+        for (int st = 0; st < kStages && prod.ok; ++st) {
+            issue(P, st, S.cg[prod.i - j0], prod, lane);
+            prod.next(S, j0, P.stage_bytes);
+        }
+        double acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+        Row rw = {};
+        int ci = -1;
+        for (int u = 0; cons.ok && good; ++u) {
+            const int st = u % kStages;
+            if (!mbar_wait(P.bar + st, (P.phase >> st) & 1u, err)) {
+                good = false;
+                break;
+            }
+            P.phase ^= 1u << st;
+            const CgView& d = S.cg[cons.i - j0];
+            if (cons.i != ci) {
+                if (ci >= 0) flush<NV>(S, warp, lane, ci - j0, acc);
+                ci = cons.i;
+            }
+            if (cons.k0 == 0) rw = Row{};
+            const int cnt = cons.count();
+            unit(cons.i, d, cons.ls, cnt, P.buf + (size_t)st * P.stage_bytes, rw);
+            if (cons.k0 + cnt >= cons.w) end(cons.i, d, cons.ls, rw, acc);
+            __syncwarp();   // every lane is done with this stage's buffer
+            if (prod.ok) {
+                issue(P, st, S.cg[prod.i - j0], prod, lane);
+                prod.next(S, j0, P.stage_bytes);
+            }
+            cons.next(S, j0, P.stage_bytes);
+        }
+        if (ci >= 0) flush<NV>(S, warp, lane, ci - j0, acc);
+        __syncthreads();
+        for (int j = threadIdx.x; j < j1 - j0; j += blockDim.x) {
+            const int i2 = j0 + j;
+            if (S.pre[i2 + 1] == S.pre[i2]) continue;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double t = 0.0;
+                for (int w = 0; w < kCgWarps; ++w) t += S.wp[(w * kBatchMaxPerBlock + j) * 2 + v];
+                parts[((size_t)v * n + i2) * nb + b] = t;
+            }
+        }
+    }
+    return good;
+}
+
+// one staged unit of the right-hand side (entries in slice order, the same
+// float64 accumulation sequence as rhs_slice)
+template <bool DC, bool AS, bool LG>
+__device__ __forceinline__ void rhs_unit(const CgView& d, int step, int64_t ls, int nk, const unsigned char* buf,
+                                         Row& rw, int lane) {
+    const int64_t row = ls * TCB_SLICE + lane;
+    if (row >= d.n) return;
+    const int r = (int)row;
+    const float* __restrict__ u = d.x + ring_cur(step) * d.n_pad;
+    const float* __restrict__ xp = d.x + ring_prev(step) * d.n_pad;
+    const float* __restrict__ bp = d.bp;
+    const int m = nk * TCB_SLICE;
+    const int16_t* c16 = reinterpret_cast<const int16_t*>(buf);
+    const int32_t* c32 = reinterpret_cast<const int32_t*>(buf);
+    const float* mvs = reinterpret_cast<const float*>(buf + m * (DC ? 2 : 4));
+    const float* kvs = mvs + m;
+    const float* avs = kvs + m;
+    float mb = (float)rw.v[0], ku = (float)rw.v[1];
+    double ax = rw.v[2];
+    for (int k = 0; k < nk; k += 8) {
+        int c[8];
+        float mv[8], kv[8], av[8], bc[8], uc[8], xc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const bool ok = k + j < nk;
+            const int e = (k + j) * TCB_SLICE + lane;
+            if constexpr (DC) c[j] = ok ? r + (int)c16[e] : r;
+            else c[j] = ok ? c32[e] : r;
+            mv[j] = ok ? mvs[e] : 0.0f;
+            kv[j] = ok ? kvs[e] : 0.0f;
+            if constexpr (AS) av[j] = __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]);
+            else av[j] = ok ? avs[e] : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            bc[j] = __ldg(bp + c[j]);
+            uc[j] = __ldg(u + c[j]);
+            if constexpr (LG) xc[j] = __ldg(xp + c[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (k + j < nk) {
+                float xg;
+                if constexpr (LG) xg = 2.0f * uc[j] - xc[j];
+                else xg = uc[j];
+                mb = __fmaf_rn(mv[j], bc[j], mb);
+                ku = __fmaf_rn(kv[j], uc[j], ku);
+                ax += (double)av[j] * (double)xg;
+            }
+        }
+    }
+    rw.v[0] = mb;
+    rw.v[1] = ku;
+    rw.v[2] = ax;
+}
+
+// the end of a right-hand-side row (as the tail of rhs_slice)
+__device__ __forceinline__ void rhs_end(const CgView& d, int step, int64_t ls, const Row& rw, double (&acc)[2],
+                                        int lane) {
+    const int64_t row = ls * TCB_SLICE + lane;
+    if (row >= d.n) return;
+    const float* __restrict__ u = d.x + ring_cur(step) * d.n_pad;
+    const float rhs = (float)rw.v[0] - (float)rw.v[1];   // float32 sums carried in the row state
+    const float ui = __ldg(u + row);
+    const float xg0 = d.linear_guess ? 2.0f * ui - __ldg(d.x + ring_prev(step) * d.n_pad + row) : ui;
+    __stwb(d.x + ring_next(step) * d.n_pad + row, xg0);
+    const float r32 = (float)((double)rhs - rw.v[2]);
+    const float di = __ldg(d.dinv + row);
+    const float z32 = (float)((double)di * (double)r32);
+    __stwb(d.r + row, r32);
+    __stwb(d.z + row, z32);
+    const double db = (double)di * (double)rhs;
+    acc[0] += db * db;
+    acc[1] += (double)r32 * (double)z32;
+}
+
+// one staged unit of A p (p formed on the fly from the gathered z and old p)
+template <bool DC, bool FIRST>
+__device__ __forceinline__ void ap_unit(const CgView& d, const float* pin, float beta, int64_t ls, int nk,
+                                        const unsigned char* buf, Row& rw, int lane) {
+    const int64_t row = ls * TCB_SLICE + lane;
+    if (row >= d.n) return;
+    const int r = (int)row;
+    const int m = nk * TCB_SLICE;
+    const int16_t* c16 = reinterpret_cast<const int16_t*>(buf);
+    const int32_t* c32 = reinterpret_cast<const int32_t*>(buf);
+    const float* avs = reinterpret_cast<const float*>(buf + m * (DC ? 2 : 4));
+    const float* z = d.z;
+    double a = rw.v[0];
+    for (int k = 0; k < nk; k += 8) {
+        int c[8];
+        float av[8], zc[8], pc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const bool ok = k + j < nk;
+            const int e = (k + j) * TCB_SLICE + lane;
+            if constexpr (DC) c[j] = ok ? r + (int)c16[e] : r;
+            else c[j] = ok ? c32[e] : r;
+            av[j] = ok ? avs[e] : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            zc[j] = __ldca(z + c[j]);
+            pc[j] = FIRST ? 0.0f : __ldca(pin + c[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (k + j < nk) a += (double)av[j] * (double)p_update(zc[j], pc[j], beta, FIRST);
+    }
+    rw.v[0] = a;
+}
+
+__device__ __forceinline__ void ap_end(const CgView& d, const float* pin, float* pout, float beta, bool first,
+                                       int64_t ls, const Row& rw, double (&acc)[1], int lane) {
+    const int64_t row = ls * TCB_SLICE + lane;
+    if (row >= d.n) return;
+    const float pn = p_update(__ldca(d.z + row), first ? 0.0f : __ldca(pin + row), beta, first);
+    __stwb(pout + row, pn);
+    const float a32 = (float)rw.v[0];
+    __stwb(d.ap + row, a32);
+    acc[0] += (double)pn * (double)a32;
+}
+
 // every block: totals of every active simulation (warp per simulation, lanes over its blocks)
 template <int NV, class F>
 __device__ __forceinline__ void totals(const BatchWS* W, BatchShared& S, const double* parts, F&& consume) {
@@ -334,17 +677,43 @@ __device__ __forceinline__ void totals(const BatchWS* W, BatchShared& S, const d
     __syncthreads();
 }
 
+// bytes of the shared carve-out before the staging area (128-byte aligned)
+__host__ __device__ inline size_t carve_bytes(int n) {
+    const size_t b = (size_t)n * (4 * sizeof(double) + 6 * sizeof(int)) +
+                     sizeof(double) * kCgWarps * kBatchMaxPerBlock * 2 + sizeof(int64_t) * (n + 1) +
+                     sizeof(int64_t) * (kBatchMaxBlocks + 1) + sizeof(CgView) * kBatchMaxPerBlock;
+    return (b + 127) / 128 * 128;
+}
+constexpr size_t kStageBarBytes = 128 * ((kCgWarps * kStages * 8 + 127) / 128);
+
 // PER_SM: blocks per SM the register budget is sized for (1: 128 registers a
-// thread, no spills; 2: 64 registers, twice the warps to hide latency)
-template <int PER_SM>
-__global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const BatchWS* __restrict__ W) {
-    extern __shared__ double smd[];
+// thread, no spills; 2: 64 registers, twice the warps to hide latency).
+// STAGED: the right-hand side and A p stream their ELL blocks through shared
+// memory by bulk copies (stage_bytes per warp and stage; 1 block per SM).
+template <int PER_SM, bool STAGED>
+__global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const BatchWS* __restrict__ W,
+                                                                       int stage_bytes) {
+    extern __shared__ __align__(128) double smd[];
     const int n = W->n;
     BatchShared S = carve(smd, n, gridDim.x);
     const int lane = threadIdx.x & 31;
     double* parts0 = W->parts;
     double* parts1 = W->parts + 2 * (size_t)n * gridDim.x;
     int32_t* err = W->err;
+    Pipe P = {};
+    if constexpr (STAGED) {
+        unsigned char* base = reinterpret_cast<unsigned char*>(smd) + carve_bytes(n);
+        const int warp = threadIdx.x >> 5;
+        P.bar = reinterpret_cast<uint64_t*>(base) + warp * kStages;
+        P.buf = base + kStageBarBytes + (size_t)warp * kStages * stage_bytes;
+        P.stage_bytes = stage_bytes;
+        P.phase = 0;
+        if (lane == 0) {
+            for (int st = 0; st < kStages; ++st) mbar_init(P.bar + st);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+    }
 
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int64_t st = W->dev[i].counter[0];
@@ -357,6 +726,26 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
 
     // ---- right-hand side, guess, r0, z0 (solver.py:46-55; monodomain.py:130-131)
     int64_t A = active_prefix(S, n, S.step);
+    if constexpr (STAGED) {
+        sweep_staged<2, RhsStreams>(
+            W, S, parts0, P, err,
+            [&](int i, const CgView& d, int64_t ls, int nk, const unsigned char* buf, Row& rw) {
+                const int step = S.step[i];
+                switch ((d.dcol ? 4 : 0) | (d.a_split ? 2 : 0) | (d.linear_guess ? 1 : 0)) {
+                    case 0: rhs_unit<false, false, false>(d, step, ls, nk, buf, rw, lane); break;
+                    case 1: rhs_unit<false, false, true>(d, step, ls, nk, buf, rw, lane); break;
+                    case 2: rhs_unit<false, true, false>(d, step, ls, nk, buf, rw, lane); break;
+                    case 3: rhs_unit<false, true, true>(d, step, ls, nk, buf, rw, lane); break;
+                    case 4: rhs_unit<true, false, false>(d, step, ls, nk, buf, rw, lane); break;
+                    case 5: rhs_unit<true, false, true>(d, step, ls, nk, buf, rw, lane); break;
+                    case 6: rhs_unit<true, true, false>(d, step, ls, nk, buf, rw, lane); break;
+                    default: rhs_unit<true, true, true>(d, step, ls, nk, buf, rw, lane); break;
+                }
+            },
+            [&](int i, const CgView& d, int64_t ls, const Row& rw, double (&acc)[2]) {
+                rhs_end(d, S.step[i], ls, rw, acc, lane);
+            });
+    } else
     sweep<2>(W, S, parts0, [&](int i, const CgView& d, int64_t ls, double (&acc)[2]) {
         const int step = S.step[i];
         switch ((d.dcol ? 4 : 0) | (d.a_split ? 2 : 0) | (d.linear_guess ? 1 : 0)) {
@@ -383,10 +772,29 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
         if (A == 0) break;
         const bool first_pass = pass == 0;
         // ---- p = z + beta p (on the fly), Ap, p.Ap
+        if constexpr (STAGED) {
+            sweep_staged<1, ApStreams>(
+                W, S, parts1, P, err,
+                [&](int i, const CgView& d, int64_t ls, int nk, const unsigned char* buf, Row& rw) {
+                    const float* pin = (pass & 1) ? d.p2 : d.p;
+                    const float beta = (float)S.be[i];
+                    if (d.dcol) {
+                        if (first_pass) ap_unit<true, true>(d, pin, beta, ls, nk, buf, rw, lane);
+                        else ap_unit<true, false>(d, pin, beta, ls, nk, buf, rw, lane);
+                    } else {
+                        if (first_pass) ap_unit<false, true>(d, pin, beta, ls, nk, buf, rw, lane);
+                        else ap_unit<false, false>(d, pin, beta, ls, nk, buf, rw, lane);
+                    }
+                },
+                [&](int i, const CgView& d, int64_t ls, const Row& rw, double (&acc)[1]) {
+                    ap_end(d, (pass & 1) ? d.p2 : d.p, (pass & 1) ? d.p : d.p2, (float)S.be[i], first_pass, ls, rw, acc,
+                           lane);
+                });
+        } else
         sweep<1>(W, S, parts1, [&](int i, const CgView& d, int64_t ls, double (&acc)[1]) {
             const float* pin = (pass & 1) ? d.p2 : d.p;
             float* pout = (pass & 1) ? d.p : d.p2;
-            const double beta = S.be[i];
+            const float beta = (float)S.be[i];
             if (d.dcol) {
                 if (first_pass) ap_slice<true, true>(d, pin, pout, beta, ls, lane, acc);
                 else ap_slice<true, false>(d, pin, pout, beta, ls, lane, acc);
@@ -439,20 +847,18 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
 
 }  // namespace
 
-size_t batch_cg_smem(int n) {
-    return (size_t)n * (4 * sizeof(double) + 6 * sizeof(int)) + sizeof(double) * kCgWarps * kBatchMaxPerBlock * 2 +
-           sizeof(int64_t) * (n + 1) + sizeof(int64_t) * (kBatchMaxBlocks + 1) + sizeof(CgView) * kBatchMaxPerBlock +
-           64;
-}
+size_t batch_cg_smem(int n) { return carve_bytes(n); }
 
-template <int PER_SM>
+namespace {
+
+template <int PER_SM, bool STAGED>
 int max_blocks(size_t smem) {
     int dev = 0, sms = 0, occ = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaFuncSetAttribute(batch_cg_kernel<PER_SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_cg_kernel<PER_SM>, kCgThreads, smem) !=
+    if (cudaFuncSetAttribute(batch_cg_kernel<PER_SM, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_cg_kernel<PER_SM, STAGED>, kCgThreads, smem) !=
             cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -462,11 +868,35 @@ int max_blocks(size_t smem) {
     return cap > kBatchMaxBlocks ? kBatchMaxBlocks : cap;
 }
 
-int batch_cg_max_blocks(size_t smem, int per_sm) {
-    return per_sm == 1 ? max_blocks<1>(smem) : per_sm == 2 ? max_blocks<2>(smem) : 0;
+}  // namespace
+
+// Staging bytes per warp and stage for n simulations (0 if the staged variant
+// does not fit): as much as shared memory allows, at most 8 KB, in whole KB.
+int batch_cg_stage_bytes(int n) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const long avail = (long)optin - (long)carve_bytes(n) - (long)kStageBarBytes - 1024;
+    long per = avail / (kCgWarps * kStages) / 1024 * 1024;
+    if (per > 8192) per = 8192;
+    return per >= 2048 ? (int)per : 0;
 }
 
-int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int per_sm, cudaStream_t s) {
+size_t batch_cg_smem_variant(int n, int variant) {
+    if (variant != 3) return carve_bytes(n);
+    return carve_bytes(n) + kStageBarBytes + (size_t)kCgWarps * kStages * batch_cg_stage_bytes(n);
+}
+
+int batch_cg_max_blocks(size_t smem, int variant) {
+    switch (variant) {
+        case 1: return max_blocks<1, false>(smem);
+        case 2: return max_blocks<2, false>(smem);
+        case 3: return max_blocks<1, true>(smem);
+    }
+    return 0;
+}
+
+int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int stage_bytes, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nb);
     cfg.blockDim = dim3(kCgThreads);
@@ -477,10 +907,12 @@ int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int per_sm, cuda
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (per_sm == 1)
-        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<1>, ws_dev));
+    if (variant == 1)
+        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<1, false>, ws_dev, 0));
+    else if (variant == 2)
+        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<2, false>, ws_dev, 0));
     else
-        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<2>, ws_dev));
+        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<1, true>, ws_dev, stage_bytes));
     return TCB_OK;
 }
 

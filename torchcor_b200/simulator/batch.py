@@ -30,7 +30,7 @@ class MonodomainBatch:
         self._structs = None
         self.sims = []
         self._dirty = True
-        self._cg_per_sm = None
+        self._cg_variant = None
 
     def add(self, sim, a_tol=1e-5, r_tol=1e-5, max_iter=100, calculate_AT_RT=True, linear_guess=True,
             snapshot_interval=1):
@@ -59,22 +59,33 @@ class MonodomainBatch:
         self._structs = arr
         lib = _lib.load()
         check(lib.tcb_batch_prepare(arr, n, self._ws.data_ptr(), self._ws.numel(), C.byref(self._plan)))
-        if self._cg_per_sm is not None:
-            check(lib.tcb_batch_set_cg(C.byref(self._plan), int(self._cg_per_sm)))
+        if self._cg_variant is not None:
+            st = lib.tcb_batch_set_cg(C.byref(self._plan), int(self._cg_variant))
+            if st != 0 and self._cg_variant == 3:   # staged variant not possible for these arrays
+                self._cg_variant = None
+            else:
+                check(st)
         self._dirty = False
 
-    def set_cg(self, per_sm):
-        """Use the batched CG kernel variant sized for ``per_sm`` (1 or 2) blocks per SM."""
-        if per_sm not in (1, 2):
-            raise ValueError("per_sm must be 1 or 2")
-        self._cg_per_sm = per_sm
+    def set_cg(self, variant):
+        """Use batched CG kernel variant 1 or 2 (streaming, sized for 1 or 2 blocks
+        per SM) or 3 (ELL streams staged in shared memory by bulk copies)."""
+        if variant not in (1, 2, 3):
+            raise ValueError("variant must be 1, 2 or 3")
+        self._cg_variant = variant
         if self.sims and not self._dirty:
-            check(_lib.load().tcb_batch_set_cg(C.byref(self._plan), int(per_sm)))
+            check(_lib.load().tcb_batch_set_cg(C.byref(self._plan), int(variant)))
+
+    def cg_variants(self):
+        """The CG variants this batch can use (3 needs 16-byte aligned ELL arrays)."""
+        if self._dirty and self.sims:
+            self._prepare()
+        return (2, 1, 3) if self._plan.cg_stage_ok else (2, 1)
 
     def autotune(self, steps=10, cache=None, force=False):
         """Choose the batched CG variant for this batch's shape on this GPU
         (cached; on a miss it times real steps of the batch, see
-        ``torchcor_b200.tune.tune_batch``).  Returns the blocks-per-SM choice."""
+        ``torchcor_b200.tune.tune_batch``).  Returns the chosen variant."""
         from torchcor_b200.tune import tune_batch
         if self._dirty and self.sims:
             self._prepare()
@@ -82,10 +93,10 @@ class MonodomainBatch:
 
     @property
     def cg_config(self):
-        """(blocks per SM, CG blocks) of the current plan."""
+        """(CG variant, CG blocks) of the current plan."""
         if self._dirty and self.sims:
             self._prepare()
-        return int(self._plan.cg_per_sm), int(self._plan.cg_blocks)
+        return int(self._plan.cg_variant), int(self._plan.cg_blocks)
 
     def step(self, n_steps=1):
         """Advance every unfinished simulation by ``n_steps`` steps (asynchronous)."""

@@ -1,9 +1,11 @@
 """Autotuning of launch choices, with the choices cached on disk.
 
 The one runtime choice that depends on the hardware and on the shape of the
-work is the batched CG kernel variant: sized for 2 blocks per SM (64 registers a
-thread, twice the warps to hide memory latency) or for 1 block per SM (128
-registers, no spills).  ``tune_batch`` times each candidate on the batch's own
+work is the batched CG kernel variant: 2 = streaming, sized for 2 blocks per SM
+(64 registers a thread, twice the warps to hide memory latency); 1 = streaming,
+1 block per SM (128 registers, no spills); 3 = 1 block per SM with the sliced-ELL
+streams staged in shared memory by bulk asynchronous copies (only where every
+ELL array is 16-byte aligned).  ``tune_batch`` times each candidate on the batch's own
 steps -- real steps that advance every simulation, so nothing is wasted -- and
 keeps the fastest; the choice is stored under a key made of the device and a
 coarse signature of the batch (log2 buckets of total nodes and of the number of
@@ -23,7 +25,7 @@ from pathlib import Path
 
 import torch
 
-CG_VARIANTS = (2, 1)   # blocks per SM of the batched CG kernel, default first
+CG_VARIANTS = (2, 1, 3)   # batched CG kernel variants, default first
 
 
 def cache_path() -> Path:
@@ -80,9 +82,9 @@ def tune_batch(batch, steps=10, cache=None, force=False):
 
     Uses the cached choice when there is one (unless ``force``); otherwise runs
     ``steps`` real batch steps with each candidate after one untimed step, keeps
-    the fastest and records it.  Needs ``(steps + 1) * len(CG_VARIANTS)`` steps
+    the fastest and records it.  Needs ``(steps + 1) * len(candidates)`` steps
     left in every simulation; with fewer it keeps the default and records
-    nothing.  Returns ``(blocks_per_sm, timings_ms_per_step or None)``."""
+    nothing.  Returns ``(variant, timings_ms_per_step or None)``."""
     cache = cache if cache is not None else TuneCache()
     sims = batch.sims
     if not sims:
@@ -90,14 +92,16 @@ def tune_batch(batch, steps=10, cache=None, force=False):
     key = batch_key(batch.device, [s._sim["struct"].n_nodes for s in sims], [s.ionic_model.name for s in sims])
     hit = None if force else cache.get(key)
     if hit is not None:
-        batch.set_cg(int(hit["cg_per_sm"]))
-        return int(hit["cg_per_sm"]), None
-    need = (steps + 1) * len(CG_VARIANTS)
+        if int(hit["cg_variant"]) in batch.cg_variants():
+            batch.set_cg(int(hit["cg_variant"]))
+            return int(hit["cg_variant"]), None
+    candidates = batch.cg_variants()
+    need = (steps + 1) * len(candidates)
     if min(s.nt + 1 - s._sim["next_step"] for s in sims) < need:
         return batch.cg_config[0], None
     stream = torch.cuda.current_stream(batch.device)
     times = {}
-    for v in CG_VARIANTS:
+    for v in candidates:
         batch.set_cg(v)
         batch.step(1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -109,5 +113,5 @@ def tune_batch(batch, steps=10, cache=None, force=False):
         times[v] = e0.elapsed_time(e1) / steps
     best = min(times, key=times.get)
     batch.set_cg(best)
-    cache.put(key, {"cg_per_sm": best, "ms_per_step": {str(k): v for k, v in times.items()}})
+    cache.put(key, {"cg_variant": best, "ms_per_step": {str(k): v for k, v in times.items()}})
     return best, times
