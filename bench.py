@@ -203,7 +203,19 @@ def tcb_arm(a, wl, world, rank, local):
     sim.run_steps(a.warmup)
     torch.cuda.synchronize(dev)
     lib = _lib.load()
-    _lib.check(lib.tcb_mono_check(C.byref(sim._sim["struct"]), stream.cuda_stream))
+    st = sim._sim["struct"]
+    _lib.check(lib.tcb_mono_check(C.byref(st), stream.cuda_stream))
+    cg_name = "cg_resident_kernel" if lib.tcb_mono_cg_kernel(C.byref(st)) == 1 else "cg_kernel"
+    # per-kernel event times for the roofline: steps warmup+1 .. warmup+profile_steps,
+    # each kernel bracketed by events on the launch stream (the same steps every run,
+    # so an ncu capture of them measures the same launches)
+    msi, msc = C.c_double(0.0), C.c_double(0.0)
+    s0 = sim._sim["next_step"]
+    _lib.check(lib.tcb_mono_profile(C.byref(st), s0, s0 + a.profile_steps, stream.cuda_stream,
+                                    C.byref(msi), C.byref(msc)))
+    sim._sim["next_step"] = s0 + a.profile_steps
+    p_iters = sim._sim["step_iters"][s0: s0 + a.profile_steps].sum().item()
+    kp = p_iters / a.profile_steps + 1.0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         torch.distributed.barrier()
@@ -219,17 +231,10 @@ def tcb_arm(a, wl, world, rank, local):
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
-    _lib.check(lib.tcb_mono_check(C.byref(sim._sim["struct"]), stream.cuda_stream))
-    iters = sim._sim["step_iters"][a.warmup + 1: a.warmup + a.steps + 1].sum().item()
+    _lib.check(lib.tcb_mono_check(C.byref(st), stream.cuda_stream))
+    t0s = a.warmup + a.profile_steps
+    iters = sim._sim["step_iters"][t0s + 1: t0s + a.steps + 1].sum().item()
     k_loop = iters / a.steps + 1.0                    # CG loop passes per step (n_iter + 1)
-    # per-kernel event times for the roofline (separate pass, same stream)
-    msi, msc = C.c_double(0.0), C.c_double(0.0)
-    s0 = sim._sim["next_step"]
-    _lib.check(lib.tcb_mono_profile(C.byref(sim._sim["struct"]), s0, s0 + a.profile_steps, stream.cuda_stream,
-                                    C.byref(msi), C.byref(msc)))
-    sim._sim["next_step"] = s0 + a.profile_steps
-    p_iters = sim._sim["step_iters"][s0: s0 + a.profile_steps].sum().item()
-    kp = p_iters / a.profile_steps + 1.0
     b_ion, b_rhs, b_iter = algorithmic_bytes(sys_.n, sys_.nnz, sim.ionic_model.state.shape[0])
     t_ion = msi.value / a.profile_steps * 1e-3
     t_cg = msc.value / a.profile_steps * 1e-3
@@ -239,11 +244,14 @@ def tcb_arm(a, wl, world, rank, local):
     gbs_ion = b_ion / t_ion / 1e9
     step_bytes = b_ion + b_rhs + k_loop * b_iter
     value = world * wl.n_nodes * a.steps / (ms / 1e3)
-    dominant = ("cg_kernel", gbs_cg, cg_bytes) if t_cg >= t_ion else ("mono_ionic_kernel", gbs_ion, b_ion)
+    dominant = (cg_name, gbs_cg, cg_bytes) if t_cg >= t_ion else ("mono_ionic_kernel", gbs_ion, b_ion)
+    # DRAM traffic per launch of the dominant kernel over the same profile steps,
+    # from an ncu capture (profiles/traffic.json; the capture command is stored there)
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get(dominant[0])
+        rec = json.loads(tf.read_text()).get(wl.name, {}).get(dominant[0])
+        traffic = rec.get("bytes_per_launch") if isinstance(rec, dict) else None
     del sim
     torch.cuda.empty_cache()
 
@@ -295,8 +303,9 @@ def tcb_arm(a, wl, world, rank, local):
         "roofline": {"bound": "hbm", "kernel": dominant[0], "achieved": dominant[1], "peak": peak,
                      "unit": "GB/s", "frac": dominant[1] / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} HBM copy bandwidth",
-                     "kernels": {"cg_kernel": {"ms_per_launch": 1e3 * t_cg, "bytes": cg_bytes, "GB/s": gbs_cg,
-                                               "cg_loop_passes": kp},
+                     "profile_steps": [a.warmup + 1, a.warmup + a.profile_steps],
+                     "kernels": {cg_name: {"ms_per_launch": 1e3 * t_cg, "bytes": cg_bytes, "GB/s": gbs_cg,
+                                           "cg_loop_passes": kp},
                                  "mono_ionic_kernel": {"ms_per_launch": 1e3 * t_ion, "bytes": b_ion,
                                                        "GB/s": gbs_ion}},
                      "step": {"bytes": step_bytes, "GB/s": step_bytes / (ms / a.steps * 1e-3) / 1e9}},
@@ -357,6 +366,13 @@ def batch_arm(a, world, rank, local):
     sizes = torch.tensor([s._sim["struct"].n_nodes for s in batch.sims], device=its.device, dtype=torch.float64)
     passes_max = float((its.max(0).values + 1).double().mean().item())
     passes_node = float(((its + 1).double() * sizes[:, None]).sum().item() / (sizes.sum().item() * its.shape[1]))
+    # algorithmic bytes of the timed steps (each simulation's B_ion + B_rhs + (it+1) B_iter)
+    from torchcor_b200.workloads import algorithmic_bytes
+    step_bytes = 0.0
+    for k, s_ in enumerate(batch.sims):
+        bi, br, bt = algorithmic_bytes(s_.system.n, s_.system.nnz, s_.ionic_model.state.shape[0])
+        step_bytes += bi + br + float((its[k] + 1).double().mean().item()) * bt
+    peak, peak_kind = peaks()
     value = world * total * K / (ms / 1e3)
     del batch, replay
     torch.cuda.empty_cache()
@@ -389,6 +405,10 @@ def batch_arm(a, world, rank, local):
                        "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,
                        "setup_s": setup_s},
             "gpu_launches": 3 * K, "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "kernel": "whole batch step (ionic per model + batched CG)",
+                         "achieved": step_bytes / (ms / K * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": step_bytes / (ms / K * 1e-3) / 1e9 / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} HBM copy bandwidth", "bytes_per_step": step_bytes},
             "plain_single_path": {"value": plain, "unit": METRIC,
                                   "what": "each simulation alone through Monodomain (same steps), summed time"},
             "speedup_vs_plain": (value / plain) if plain else None}

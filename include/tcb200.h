@@ -185,6 +185,11 @@ int tcb_mono_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* 
  * ms_ionic / ms_cg (for roofline accounting; costs one event pair per launch). */
 int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream, double* ms_ionic,
                      double* ms_cg);
+/* Which CG kernel tcb_mono_run launches for this simulation on the current
+ * device: 1 = the kernel keeping each block's rows in shared memory, 0 = the
+ * streaming kernel; negative = error status.  No counterpart in the reference
+ * (used to label measurements). */
+int tcb_mono_cg_kernel(const tcb_mono* m);
 /* tcb_mono_run without scratch arguments (no counterpart in the reference):
  * for callers that cannot allocate device memory at the call site (a host
  * application that owns the device memory pool and forbids allocations after

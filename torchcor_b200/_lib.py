@@ -86,6 +86,7 @@ SIGNATURES = [
     ("tcb_mono_scratch_doubles", _i64, []),
     ("tcb_mono_run", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),
     ("tcb_mono_profile", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp, C.POINTER(_f64), C.POINTER(_f64)]),
+    ("tcb_mono_cg_kernel", C.c_int, [C.POINTER(tcb_mono)]),
     ("tcb_mono_run_noalloc", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),
     ("tcb_mono_finish", C.c_int, [C.POINTER(tcb_mono), _vp]),
     ("tcb_mono_check", C.c_int, [C.POINTER(tcb_mono), _vp]),

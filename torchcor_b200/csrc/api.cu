@@ -170,6 +170,12 @@ extern "C" int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t s
     return rc;
 }
 
+extern "C" int tcb_mono_cg_kernel(const tcb_mono* m) {
+    int st = validate(m);
+    if (st) return st;
+    return cg_uses_resident(make_dev(m)) ? 1 : 0;
+}
+
 extern "C" int tcb_mono_finish(const tcb_mono* m, void* stream) {
     int st = validate(m);
     if (st) return st;

@@ -56,17 +56,19 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(MonoDev d) {
         if (row >= d.n) continue;
         const int64_t base = d.slice_ptr[s] + lane;
         const int w = (int)((d.slice_ptr[s + 1] - d.slice_ptr[s]) / TCB_SLICE);
-        double mb = 0.0, ku = 0.0, ax = 0.0;
+        // M b' and K u in float32 (the reference's float32 products), A x0 in float64
+        float mb = 0.0f, ku = 0.0f;
+        double ax = 0.0;
         for (int k = 0; k < w; ++k) {
             const int64_t e = base + (int64_t)k * TCB_SLICE;
             const int c = __ldg(d.col + e);
             const float uc = u[c];
             const float xg = lg ? 2.0f * uc - xp[c] : uc;
-            mb += (double)__ldg(d.mv + e) * (double)bp[c];
-            ku += (double)__ldg(d.kv + e) * (double)uc;
+            mb = __fmaf_rn(__ldg(d.mv + e), bp[c], mb);
+            ku = __fmaf_rn(__ldg(d.kv + e), uc, ku);
             ax += (double)__ldg(d.av + e) * (double)xg;
         }
-        const float rhs = (float)mb - (float)ku;
+        const float rhs = mb - ku;
         const float ui = u[row];
         x[row] = lg ? 2.0f * ui - xp[row] : ui;
         const float r32 = (float)((double)rhs - ax);
@@ -188,6 +190,9 @@ int cg_blocks(const MonoDev& d) {
     int64_t nb = want < cap ? want : cap;
     return (int)(nb < 1 ? 1 : nb);
 }
+
+// 1 if launch_cg runs the shared-memory-resident kernel for this simulation, 0 if the streaming one
+int cg_uses_resident(const MonoDev& d) { return !env_is("TCB_CG_KERNEL", "streaming") && resident_blocks(d) > 0; }
 
 int launch_cg(const MonoDev& d, cudaStream_t s) {
     if (!env_is("TCB_CG_KERNEL", "streaming")) {

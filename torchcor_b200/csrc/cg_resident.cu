@@ -7,7 +7,7 @@
 //  * x, r, z, p, Ap and 1/diag of a block's rows live in shared memory
 //    (24 B per row); only z and p, which neighbouring rows read, go to global
 //    memory (L2-resident), and x once at the end;
-//  * the search-direction update p = z + beta*p is formed on the fly inside
+//  * the search-direction update p = z + beta*p (float32 fused multiply-add) is formed on the fly inside
 //    the matrix-vector product from the gathered z and previous p (the global
 //    p is double-buffered), so a CG iteration has two grid barriers (after
 //    p.Ap and after the ||z||, r.z reductions) instead of three;
@@ -49,9 +49,10 @@ __device__ __forceinline__ int col_at<int16_t>(const int16_t* __restrict__ col, 
     return (int)row + (int)__ldg(col + e);
 }
 
-// p_new = z + beta * p_old, the same float32 result for every row that forms it
-__device__ __forceinline__ float p_update(float z, float p_old, double beta, bool first) {
-    return first ? z : (float)(beta * (double)p_old + (double)z);
+// p_new = z + beta * p_old in float32 (one fused multiply-add, beta rounded to
+// float32): the same result for every row that forms it
+__device__ __forceinline__ float p_update(float z, float p_old, float beta, bool first) {
+    return first ? z : __fmaf_rn(beta, p_old, z);
 }
 
 template <typename IDX, int MINB, bool ASPLIT>
@@ -90,7 +91,10 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
         const int li = (int)((s - s_begin) * TCB_SLICE + lane);
         const int64_t base = d.slice_ptr[s] + lane;
         const int w = (int)((d.slice_ptr[s + 1] - d.slice_ptr[s]) / TCB_SLICE);
-        double mb = 0.0, ku = 0.0, ax = 0.0;
+        // M b' and K u accumulate in float32 (the reference's float32 products),
+        // A x0 in float64 (the reference's CG is float64; b - A x0 cancels)
+        float mb = 0.0f, ku = 0.0f;
+        double ax = 0.0;
         for (int k0 = 0; k0 < w; k0 += 4) {
             int c[4];
             float mv[4], kv[4], av[4];
@@ -113,12 +117,12 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const float xg = lg ? 2.0f * uc[j] - xc[j] : uc[j];
-                mb += (double)mv[j] * (double)bc[j];
-                ku += (double)kv[j] * (double)uc[j];
+                mb = __fmaf_rn(mv[j], bc[j], mb);
+                ku = __fmaf_rn(kv[j], uc[j], ku);
                 ax += (double)av[j] * (double)xg;
             }
         }
-        const float rhs = (float)mb - (float)ku;
+        const float rhs = mb - ku;
         const float ui = u[row];
         sx[li] = lg ? 2.0f * ui - xp[row] : ui;
         const float r32 = (float)((double)rhs - ax);
@@ -143,6 +147,7 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
     int it = 0;
     while (it < d.max_iter) {
         const bool first = it == 0;
+        const float beta32 = (float)beta;
         const float* pin = pg[it & 1];
         float* __restrict__ pout = pg[(it + 1) & 1];
         // ---- p = z + beta p (on the fly), Ap, p.Ap
@@ -171,9 +176,9 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
                     pc[j] = first ? 0.0f : pin[c[j]];
                 }
 #pragma unroll
-                for (int j = 0; j < 8; ++j) a += (double)av[j] * (double)p_update(zc[j], pc[j], beta, first);
+                for (int j = 0; j < 8; ++j) a += (double)av[j] * (double)p_update(zc[j], pc[j], beta32, first);
             }
-            const float pn = p_update(sz[li], first ? 0.0f : sp[li], beta, first);
+            const float pn = p_update(sz[li], first ? 0.0f : sp[li], beta32, first);
             sp[li] = pn;
             pout[row] = pn;
             const float a32 = (float)a;

@@ -42,5 +42,6 @@ int launch_mono_finish(const MonoDev& d, cudaStream_t s);
 int launch_cg(const MonoDev& d, cudaStream_t s);
 int launch_cg_resident(const MonoDev& d, cudaStream_t s);
 int resident_blocks(const MonoDev& d);
+int cg_uses_resident(const MonoDev& d);
 
 }  // namespace tcb
