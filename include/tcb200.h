@@ -180,6 +180,13 @@ int64_t tcb_mono_scratch_doubles(void);
  * counter).  Non-convergence is not an error (n_iter == max_iter), as in the
  * reference. */
 int tcb_mono_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream);
+/* The linear solves alone for steps [step_begin, step_end): right-hand side
+ * M b' - K' u, linear-extrapolation guess from the solution ring, Jacobi-PCG
+ * (replaces ConjugateGradient.solve, solver.py:40-76, where the caller supplies
+ * b' and the matrices); the ionic kernel is not run.  Used for the extracellular
+ * potential recovery (monodomain.py:254-286) with M := K(sigma_i), b' := -Vm,
+ * K' := 0, A := K(sigma_i + sigma_e). */
+int tcb_mono_cg_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream);
 /* Like tcb_mono_run, recording CUDA events around every kernel on `stream`;
  * adds the summed device times (ms) of the ionic and CG kernels to
  * ms_ionic / ms_cg (for roofline accounting; costs one event pair per launch). */

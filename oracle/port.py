@@ -841,6 +841,30 @@ class Monodomain:
         self.system = build_system(self.nodes, self.elems, sm, self.dt, self.dtype, self.Chi, self.Cm, self.theta)
         self.cg = PCG(self.system.PC, self.system.A, dtype=torch.float64)
 
+    def phie_recovery(self, Vm, a_tol=1e-5, r_tol=1e-5, max_iter=100):   # :254-286
+        """Extracellular potential of every Vm frame: K(sigma_i + sigma_e) phi = -K(sigma_i) V
+        by Jacobi-PCG in float64 with the linear-extrapolation guess across frames, then
+        phi -= mean(phi) in place on the returned tensor (which, for float64 frames, is the
+        solver's own x, as in the reference)."""
+        si, se, _ = self.conductivity.sigma(self.fibres)
+        local = tri_surface_local_matrices if self.elems.shape[1] == 3 else tet_local_matrices
+        n = self.nodes.shape[0]
+        Me, Ke = local(self.nodes, self.elems, si + se, self.dtype)
+        K_ie, _ = scatter_coo(self.elems, Me, Ke, n, self.dtype)
+        Me, Ke = local(self.nodes, self.elems, si, self.dtype)
+        K_i, _ = scatter_coo(self.elems, Me, Ke, n, self.dtype)
+        cg = PCG(jacobi(K_ie), K_ie.to_sparse_csr(), dtype=torch.float64)
+        cg.initialize(x=torch.zeros_like(Vm[0]), linear_guess=True)
+        K_i = K_i.to_sparse_csr()
+        out, iters = [], []
+        for i in range(Vm.shape[0]):
+            b = -K_i @ Vm[i, :]
+            phi, it = cg.solve(b, a_tol=a_tol, r_tol=r_tol, max_iter=max_iter)
+            phi -= phi.mean()
+            out.append(phi)
+            iters.append(it)
+        return torch.stack(out, dim=0), iters
+
     def step(self, u, t, a_tol, r_tol, max_iter):           # :109-139
         du = self.ionic.differentiate(u) / 100
         b = u * self.Cm + self.dt * du

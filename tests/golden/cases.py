@@ -52,7 +52,7 @@ CASES = [
          conductivity=[dict(region_ids=[1], il=0.17, it=0.019, el=0.62, et=0.2)],
          stimuli=[dict(file="face.vtx", nodes=dict(type="face", axis=2, side=1), start=0.0, duration=1.0,
                        intensity=100, period=4.0, count=2)],
-         dt=0.01, T=12.0, tol=1e-5, max_iter=100, full_matrices=True),
+         dt=0.01, T=12.0, tol=1e-5, max_iter=100, full_matrices=True, phie=True),
     # long enough for repolarisation times (RT) to be set
     dict(kind="tissue", name="cube4_ms_rt_f32", model="ms", dtype="f32",
          mesh=dict(type="cube", n=4, h=0.5, fibres="x", regions="one"), conductivity=_ONE, stimuli=_FACE,

@@ -100,6 +100,9 @@ def run_tissue(md, ionic, case, workdir):
     total = sim.solve(a_tol=case["tol"], r_tol=case["tol"], max_iter=case["max_iter"], calculate_AT_RT=True,
                       linear_guess=True, snapshot_interval=1, verbose=False, result_path=str(out_dir))
     wall = time.time() - t0
+    if case.get("phie"):
+        # extracellular potential recovery from the saved Vm frames (monodomain.py:254-286)
+        sim.phie_recovery(a_tol=case["tol"], r_tol=case["tol"], max_iter=case["max_iter"])
     AT = torch.load(out_dir / "ATs.pt").numpy()
     RT = torch.load(out_dir / "RTs.pt").numpy()
     Vm = torch.load(out_dir / "Vm.pt").numpy()
@@ -124,6 +127,8 @@ def run_tissue(md, ionic, case, workdir):
         fx["A_sum"] = np.float64(sim.A.values().double().sum())
     if traj:
         fx["traj"] = torch.stack(traj).numpy()
+    if case.get("phie"):
+        fx["Phi_e"] = torch.load(out_dir / "Phi_e.pt").numpy()
     st = states_of(im, case["model"])
     if case.get("keep_states"):
         for k, v in st.items():

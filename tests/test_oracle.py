@@ -63,3 +63,16 @@ def test_oracle_golden_pins_exist():
     # every case declared has a fixture
     for c in C.CASES:
         assert (golden(c["name"]) is not None)
+
+
+def test_oracle_phie_recovery(tmp_path):
+    """Extracellular potential recovery (monodomain.py:254-286) from the solve's Vm
+    frames, on the case with intracellular and extracellular conductivities."""
+    torch.set_num_threads(8)
+    case = C.case("cube4_ms_period_f32")
+    g = golden(case["name"])
+    sim, r = run_oracle_tissue(case, case_mesh_dir(case, tmp_path))
+    phi, iters = sim.phie_recovery(r.Vm, a_tol=case["tol"], r_tol=case["tol"], max_iter=case["max_iter"])
+    ref = g["Phi_e"]
+    assert phi.shape == ref.shape
+    assert np.abs(phi.numpy() - ref).max() <= 1e-5 * np.abs(ref).max()

@@ -85,6 +85,7 @@ SIGNATURES = [
     ("tcb_model_differentiate", C.c_int, [_i32, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp]),
     ("tcb_mono_scratch_doubles", _i64, []),
     ("tcb_mono_run", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),
+    ("tcb_mono_cg_run", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),
     ("tcb_mono_profile", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp, C.POINTER(_f64), C.POINTER(_f64)]),
     ("tcb_mono_cg_kernel", C.c_int, [C.POINTER(tcb_mono)]),
     ("tcb_mono_run_noalloc", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),

@@ -144,6 +144,61 @@ def assemble_system(nodes, elems_np, sl, st, fibres, dt, chi=140, cm=0.01, theta
                   sell_m=sell[0], sell_k=sell[1], sell_a=sell[2], sell_dcol=dcol, a_split=bool(a_split.item()))
 
 
+def assemble_phie(nodes, elems_np, sl_i, st_i, sl_e, st_e, fibres) -> System:
+    """Matrices of the extracellular potential recovery (monodomain.py:254-286)
+    in the solver's layout: M := K(sigma_i), K' := 0, A := K(sigma_i + sigma_e)
+    (each sigma formed per element as st I + (sl - st) f f^T), 1/diag(A).
+    A is produced by the monodomain system kernel with Cm = 0, chi = theta = dt = 1,
+    which returns K(sigma_i + sigma_e) exactly and a zero K'."""
+    lib = _lib.load()
+    dev = nodes.device
+    n = nodes.shape[0]
+    n_pad = n_padded(n)
+    pat = build_pattern(elems_np, n)
+    nnz, k = pat.nnz, pat.k
+    elems = torch.from_numpy(np.ascontiguousarray(elems_np, dtype=np.int32)).to(dev)
+    slot_ptr = torch.from_numpy(pat.slot_ptr).to(dev)
+    slot_src = torch.from_numpy(pat.slot_src).to(dev)
+    s = stream_ptr()
+
+    def stiffness(sl, st):
+        ke, mw = local_matrices(nodes, elems, sl.contiguous(), st.contiguous(), fibres)
+        kv = torch.empty(nnz, device=dev, dtype=torch.float32)
+        mv = torch.empty(nnz, device=dev, dtype=torch.float32)
+        check(lib.tcb_assemble_gather(k, ptr(slot_ptr), ptr(slot_src), nnz, ptr(ke), ptr(mw), ptr(kv), ptr(mv), s))
+        return kv, mv
+
+    kie, mass = stiffness(sl_i + sl_e, st_i + st_e)
+    ki, _ = stiffness(sl_i, st_i)
+    diag = torch.from_numpy(pat.diag).to(dev)
+    a_val = torch.empty(nnz, device=dev, dtype=torch.float32)
+    zero = torch.empty(nnz, device=dev, dtype=torch.float32)
+    d_inv = torch.empty(n_pad, device=dev, dtype=torch.float32)
+    check(lib.tcb_assemble_system(nnz, n, n_pad, ptr(diag), ptr(kie), ptr(mass), 1.0, 0.0, 1.0, 1.0,
+                                  ptr(a_val), ptr(zero), ptr(d_inv), None, s))
+    n_slices = (n + _lib.TCB_SLICE - 1) // _lib.TCB_SLICE
+    sp = np.empty(n_slices + 1, dtype=np.int64)
+    n_entries = C.c_int64()
+    check(lib.tcb_sell_layout(ptr(pat.rowptr), n, ptr(sp), C.byref(n_entries)))
+    rowptr = torch.from_numpy(pat.rowptr).to(dev)
+    col = torch.from_numpy(pat.col).to(dev)
+    slice_ptr = torch.from_numpy(sp).to(dev)
+    ne = n_entries.value
+    sell_col = torch.empty(ne, device=dev, dtype=torch.int32)
+    sell = [torch.empty(ne, device=dev, dtype=torch.float32) for _ in range(3)]
+    vin = (C.c_void_p * 3)(ptr(ki), ptr(zero), ptr(a_val))
+    vout = (C.c_void_p * 3)(*[ptr(t) for t in sell])
+    check(lib.tcb_sell_pack(n, ptr(rowptr), ptr(col), ptr(slice_ptr), n_slices, 3, vin, ptr(sell_col), vout, s))
+    dcol = torch.empty(ne, device=dev, dtype=torch.int16)
+    mx = torch.zeros(1, device=dev, dtype=torch.int32)
+    check(lib.tcb_sell_delta(n, ptr(slice_ptr), n_slices, ptr(sell_col), ptr(dcol), ptr(mx), s))
+    if int(mx.item()) >= 32768:
+        dcol = None
+    return System(n=n, n_pad=n_pad, nnz=nnz, rowptr=rowptr, col=col, m_val=ki, k_val=kie, a_val=a_val,
+                  krhs_val=zero, d_inv=d_inv, n_slices=n_slices, slice_ptr=slice_ptr, sell_col=sell_col,
+                  sell_m=sell[0], sell_k=sell[1], sell_a=sell[2], sell_dcol=dcol, a_split=False)
+
+
 class _Matrices:
     k = 4
 

@@ -133,6 +133,20 @@ extern "C" int tcb_mono_run(const tcb_mono* m, int64_t step_begin, int64_t step_
     return TCB_OK;
 }
 
+extern "C" int tcb_mono_cg_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream) {
+    int st = validate(m);
+    if (st) return st;
+    if (step_begin < 1 || step_end > m->nt + 1 || step_begin > step_end)
+        return fail(TCB_EINVAL, "tcb_mono_cg_run: step range outside [1, nt]");
+    cudaStream_t s = as_stream(stream);
+    MonoDev d = make_dev(m);
+    for (int64_t n = step_begin; n < step_end; ++n) {
+        st = launch_cg(d, s);
+        if (st) return st;
+    }
+    return TCB_OK;
+}
+
 extern "C" int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream,
                                 double* ms_ionic, double* ms_cg) {
     int st = validate(m);

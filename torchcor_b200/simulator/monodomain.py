@@ -19,7 +19,7 @@ import torch
 
 from torchcor_b200 import _lib
 from torchcor_b200._lib import check, ptr, stream_ptr
-from torchcor_b200.core.assemble import assemble_system
+from torchcor_b200.core.assemble import assemble_phie, assemble_system
 from torchcor_b200.core.conductivity import Conductivity
 from torchcor_b200.core.mesh import MeshReader
 from torchcor_b200.core.stimulation import Stimuli
@@ -223,6 +223,79 @@ class Monodomain:
             if sim["snaps"] is not None:
                 torch.save(sim["snaps"].cpu(), rp / "Vm.pt")
         return self.n_total_iter
+
+    def phie_recovery(self, a_tol=1e-5, r_tol=1e-5, max_iter=100, Vm=None, verbose=False):
+        """Extracellular potential of every Vm frame (monodomain.py:254-286):
+        K(sigma_i + sigma_e) phi_e = -K(sigma_i) Vm, Jacobi-PCG with the linear
+        extrapolation guess from the previous frames' solutions, then phi_e minus its
+        mean.  ``Vm`` defaults to the snapshots of the last solve, else
+        ``result_path/Vm.pt``; the result is returned, kept as ``self.phi_e`` and saved
+        as ``result_path/Phi_e.pt`` when the solve had a result path.  Needs
+        intracellular and extracellular conductivities (``add_conductivity(..., el, et)``).
+        The solves run on the device (``tcb_mono_cg_run``); printing per frame, as the
+        reference does, only with ``verbose=True``."""
+        c = self.conductivity
+        if c.sigma_il is None or c.sigma_el is None:
+            raise ValueError("phie_recovery needs intracellular and extracellular conductivities "
+                             "(add_conductivity(..., el=..., et=...))")
+        if Vm is None:
+            if getattr(self, "solutions", None) is not None:
+                Vm = self.solutions
+            elif self.result_path is not None and (self.result_path / "Vm.pt").exists():
+                Vm = torch.load(self.result_path / "Vm.pt")
+            else:
+                raise ValueError("no Vm frames: solve with snapshot_interval < T first, or pass Vm")
+        dev = self.device
+        Vm = Vm.to(device=dev, dtype=torch.float32).contiguous()
+        F, n = Vm.shape
+        s = assemble_phie(self.nodes, self._elems_np, c.sigma_il.contiguous(), c.sigma_it.contiguous(),
+                          c.sigma_el.contiguous(), c.sigma_et.contiguous(), self.fibres.contiguous())
+        f32 = dict(device=dev, dtype=torch.float32)
+        n_pad = s.n_pad
+        buf = dict(x=torch.zeros((3, n_pad), **f32), bp=torch.zeros(n_pad, **f32), r=torch.zeros(n_pad, **f32),
+                   p=torch.zeros(n_pad, **f32), ap=torch.zeros(n_pad, **f32), z=torch.zeros(n_pad, **f32),
+                   p2=torch.zeros(n_pad, **f32), placeholder=torch.zeros(n_pad, **f32),
+                   flags=torch.zeros(F + 2, device=dev, dtype=torch.int32),
+                   step_t=torch.zeros(F + 2, **f32),
+                   step_iters=torch.zeros(F + 1, device=dev, dtype=torch.int32),
+                   counter=torch.tensor([1, 0, 0, 0], device=dev, dtype=torch.int32),
+                   scratch=torch.zeros(int(_lib.load().tcb_mono_scratch_doubles()), device=dev,
+                                       dtype=torch.float64),
+                   barrier=torch.zeros(4, device=dev, dtype=torch.int32),
+                   params=np.zeros(16, dtype=np.float64))
+        m = _lib.tcb_mono()
+        m.n_nodes, m.n_pad, m.n_slices, m.nt = n, n_pad, s.n_slices, F
+        m.model, m.n_states = _lib.MODEL_MS, 1          # the ionic fields are placeholders: no ionic kernel runs
+        m.slice_ptr, m.col, m.col_delta = ptr(s.slice_ptr), ptr(s.sell_col), ptr(s.sell_dcol)
+        m.m_val, m.k_val, m.a_val, m.d_inv = ptr(s.sell_m), ptr(s.sell_k), ptr(s.sell_a), ptr(s.d_inv)
+        m.state, m.tables = ptr(buf["placeholder"]), None
+        m.x, m.bprime, m.r, m.p, m.ap, m.z, m.p2 = (ptr(buf[k]) for k in ("x", "bp", "r", "p", "ap", "z", "p2"))
+        m.at = m.rt = ptr(buf["placeholder"])
+        m.snapshots = None
+        m.stim_bits, m.step_t, m.step_stim = ptr(buf["flags"]), ptr(buf["step_t"]), ptr(buf["flags"])
+        m.a_tol, m.r_tol, m.max_iter = float(a_tol), float(r_tol), int(max_iter)
+        m.linear_guess, m.at_rt, m.per_frame = 1, 0, 0
+        m.cm, m.dt = 0.0, 1.0
+        m.a_split = 0
+        m.step_iters, m.counter = ptr(buf["step_iters"]), ptr(buf["counter"])
+        m.scratch, m.barrier = ptr(buf["scratch"]), ptr(buf["barrier"])
+        m.params = buf["params"].ctypes.data
+        lib = _lib.load()
+        out = torch.empty((F, n), **f32)
+        for k in range(F):
+            buf["bp"][:n] = -Vm[k]                       # b' := -Vm so that M b' = -K(sigma_i) Vm
+            check(lib.tcb_mono_cg_run(C.byref(m), k + 1, k + 2, stream_ptr()))
+            phi = out[k]
+            phi.copy_(buf["x"][(k + 1) % 3, :n])         # the step's solution slot of the ring
+            phi -= phi.mean()
+            if verbose:
+                print(phi.min().item(), phi.max().item(), int(buf["step_iters"][k + 1].item()), flush=True)
+        check(lib.tcb_mono_check(C.byref(m), stream_ptr()))
+        self.phi_e = out
+        self.phie_iters = buf["step_iters"][1:].cpu()
+        if self.result_path is not None:
+            torch.save(out.cpu(), self.result_path / "Phi_e.pt")
+        return out
 
     def prepare(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1):
         """Assemble and set up the device state of a solve without running it
