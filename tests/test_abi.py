@@ -209,3 +209,15 @@ def test_monodomain_requires_cuda():
     from torchcor_b200.simulator import Monodomain
     with pytest.raises(RuntimeError):
         Monodomain(ModifiedMS2v(0.01, device="cpu"), T=1.0, dt=0.01, device="cpu")
+
+
+def test_rcm_order_is_a_bandwidth_reducing_permutation():
+    from torchcor_b200 import meshgen
+    from torchcor_b200.simulator.monodomain import rcm_order
+    nodes, tris = meshgen.icosphere_fast(4, 25.0)
+    p = rcm_order(tris, len(nodes))
+    assert np.array_equal(np.sort(p), np.arange(len(nodes)))
+    inv = np.empty_like(p)
+    inv[p] = np.arange(len(p))
+    bw = lambda e: max(np.abs(e[:, i] - e[:, j]).max() for i in range(3) for j in range(3))  # noqa: E731
+    assert bw(inv[tris]) * 10 < bw(tris)

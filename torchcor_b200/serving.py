@@ -104,8 +104,11 @@ def generate_requests(count=512, seed=2025, median=50_000, sigma=0.8, lo=10_000,
     return reqs
 
 
-def build_sim(req: Request, device):
-    """The ``Monodomain`` of a request (mesh, conductivities, stimuli; not yet assembled)."""
+def build_sim(req: Request, device, reorder=None):
+    """The ``Monodomain`` of a request (mesh, conductivities, stimuli; not yet assembled).
+    Icosphere nodes are renumbered by reverse Cuthill-McKee unless ``reorder=False``
+    (their subdivision numbering scatters neighbours across the whole index range);
+    the structured cubes keep their numbering."""
     from torchcor_b200.ionic import CourtemancheRamirezNattel, ModifiedMS2v, TenTusscherPanfilov
     from torchcor_b200.simulator import Monodomain
     if req.model == "ttp":
@@ -114,7 +117,9 @@ def build_sim(req: Request, device):
         im = CourtemancheRamirezNattel(req.dt, device=device)
     else:
         im = ModifiedMS2v(req.dt, device=device)
-    sim = Monodomain(im, T=req.T, dt=req.dt, device=device)
+    if reorder is None:
+        reorder = req.mesh == "ico"
+    sim = Monodomain(im, T=req.T, dt=req.dt, device=device, reorder=reorder)
     if req.mesh == "cube":
         nodes_um, elems = meshgen.cube(req.size, 0.25)
         fib = meshgen.fibres_constant(len(elems))

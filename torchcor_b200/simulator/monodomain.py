@@ -26,8 +26,21 @@ from torchcor_b200.core.stimulation import Stimuli
 from torchcor_b200.device import get_device
 
 
+def rcm_order(elems, n_nodes):
+    """Reverse Cuthill-McKee order (internal index -> node id) of the node graph
+    whose edges join the nodes of each element."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+    el = np.asarray(elems, dtype=np.int64)
+    k = el.shape[1]
+    rows = np.concatenate([el[:, i] for i in range(k) for j in range(k) if i != j])
+    cols = np.concatenate([el[:, j] for i in range(k) for j in range(k) if i != j])
+    g = sp.csr_matrix((np.ones(len(rows), dtype=np.int8), (rows, cols)), shape=(n_nodes, n_nodes))
+    return np.asarray(reverse_cuthill_mckee(g, symmetric_mode=True), dtype=np.int64)
+
+
 class Monodomain:
-    def __init__(self, ionic_model, T, dt, device=None, dtype=None):
+    def __init__(self, ionic_model, T, dt, device=None, dtype=None, reorder=False):
         self.device = torch.device(device) if device is not None else get_device()
         if self.device.type != "cuda":
             raise RuntimeError("torchcor_b200.Monodomain needs a CUDA device (no CPU fallback)")
@@ -51,6 +64,13 @@ class Monodomain:
         self.mesh_path = None
         self.result_path = None
         self._sim = None
+        # reorder=True: nodes are renumbered by reverse Cuthill-McKee for memory
+        # locality (torchcor/core/reorder.py:7-48 offers the same ordering); every
+        # per-node input and output of this class stays in the caller's numbering,
+        # only the exported M/K/A are in the internal one (node_order maps it)
+        self.reorder = bool(reorder)
+        self.node_order = None          # internal index -> caller's node id
+        self._perm_t = self._inv_t = None
 
     # ------------------------------------------------------------------ input
     def load_mesh(self, path="Data/ventricle/Case_1", unit_conversion=1000):
@@ -61,6 +81,16 @@ class Monodomain:
     def load_arrays(self, nodes, elems, regions, fibres):
         """Mesh already in memory: nodes (N,3) in mm, elems (E,3|4), per-element regions and fibres."""
         self.n_nodes = int(nodes.shape[0])
+        elems = np.ascontiguousarray(elems, dtype=np.int32)
+        if self.reorder:
+            perm = rcm_order(elems, self.n_nodes)
+            inv = np.empty_like(perm)
+            inv[perm] = np.arange(self.n_nodes, dtype=perm.dtype)
+            nodes = np.asarray(nodes)[perm]
+            elems = inv[elems].astype(np.int32)
+            self.node_order = perm
+            self._perm_t = torch.from_numpy(perm).to(self.device)
+            self._inv_t = torch.from_numpy(inv).to(self.device)
         self._elems_np = np.ascontiguousarray(elems, dtype=np.int32)
         self.nodes = torch.from_numpy(np.ascontiguousarray(nodes)).to(dtype=torch.float32, device=self.device)
         self.elems = torch.from_numpy(self._elems_np).to(device=self.device)
@@ -68,6 +98,13 @@ class Monodomain:
         self.fibres = torch.from_numpy(np.ascontiguousarray(fibres)).to(dtype=torch.float32, device=self.device)
         self.stimuli = Stimuli(self.n_nodes, self.device, self.dtype)
         self.conductivity = Conductivity(self.regions, dtype=self.dtype)
+
+    def _to_caller(self, t):
+        """Per-node tensor (last axis) from the internal numbering to the caller's."""
+        return t if t is None or self._inv_t is None else t[..., self._inv_t]
+
+    def _to_internal(self, t):
+        return t if t is None or self._perm_t is None else t[..., self._perm_t]
 
     def add_stimulus(self, vtx_filepath, start, duration, intensity, period=None, count=1, region=None):
         if period is None:
@@ -112,7 +149,7 @@ class Monodomain:
             ap=torch.zeros(n_pad, **f32), z=torch.zeros(n_pad, **f32), p2=torch.zeros(n_pad, **f32),
             at=torch.full((n,), -1.0, **f32), rt=torch.full((n,), -1.0, **f32),
             snaps=snaps, u0=u0,
-            stim_bits=torch.from_numpy(self.stimuli.membership_bits().view(np.int32)).to(dev),
+            stim_bits=torch.from_numpy(self._stim_bits().view(np.int32)).to(dev),
             step_t=torch.from_numpy(t32).to(dev), step_stim=torch.from_numpy(mask.view(np.int32)).to(dev),
             step_iters=torch.zeros(nt + 1, device=dev, dtype=torch.int32),
             counter=torch.tensor([1, 0, 0, 0], device=dev, dtype=torch.int32),
@@ -171,9 +208,14 @@ class Monodomain:
         replay.graph = graph
         return replay
 
+    def _stim_bits(self):
+        bits = self.stimuli.membership_bits()          # caller's numbering
+        return bits if self.node_order is None else np.ascontiguousarray(bits[self.node_order])
+
     def current_solution(self):
+        """Membrane potential after the last step run (caller's node numbering)."""
         sim = self._sim
-        return sim["x"][(sim["next_step"] + 2) % 3, : self.n_nodes]
+        return self._to_caller(sim["x"][(sim["next_step"] + 2) % 3, : self.n_nodes])
 
     def step(self, u, t, a_tol, r_tol, max_iter, verbose=False):
         """One step of the prepared simulation (monodomain.py:109-139).  ``u`` must be
@@ -187,7 +229,7 @@ class Monodomain:
         n = sim["next_step"]
         if n > self.nt:
             raise RuntimeError("all time steps of this simulation have been run")
-        sim["x"][(n + 2) % 3, : self.n_nodes] = u
+        sim["x"][(n + 2) % 3, : self.n_nodes] = self._to_internal(torch.as_tensor(u, device=self.device))
         sim["step_t"][n] = float(t)
         m = 0
         for k, s in enumerate(self.stimuli.stimulus_list):
@@ -211,17 +253,17 @@ class Monodomain:
         check(lib.tcb_mono_finish(C.byref(st), stream_ptr()))
         check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
         self.n_total_iter = int(sim["step_iters"].sum().item())
-        self.activation_time = sim["at"]
-        self.repolarization_time = sim["rt"]
-        self.solutions = sim["snaps"]
+        self.activation_time = self._to_caller(sim["at"])
+        self.repolarization_time = self._to_caller(sim["rt"])
+        self.solutions = self._to_caller(sim["snaps"])
         if result_path is not None:
             rp = Path(result_path)
             rp.mkdir(parents=True, exist_ok=True)
             if calculate_AT_RT:
-                torch.save(sim["at"].cpu(), rp / "ATs.pt")
-                torch.save(sim["rt"].cpu(), rp / "RTs.pt")
-            if sim["snaps"] is not None:
-                torch.save(sim["snaps"].cpu(), rp / "Vm.pt")
+                torch.save(self.activation_time.cpu(), rp / "ATs.pt")
+                torch.save(self.repolarization_time.cpu(), rp / "RTs.pt")
+            if self.solutions is not None:
+                torch.save(self.solutions.cpu(), rp / "Vm.pt")
         return self.n_total_iter
 
     def phie_recovery(self, a_tol=1e-5, r_tol=1e-5, max_iter=100, Vm=None, verbose=False):
@@ -246,7 +288,7 @@ class Monodomain:
             else:
                 raise ValueError("no Vm frames: solve with snapshot_interval < T first, or pass Vm")
         dev = self.device
-        Vm = Vm.to(device=dev, dtype=torch.float32).contiguous()
+        Vm = self._to_internal(Vm.to(device=dev, dtype=torch.float32)).contiguous()
         F, n = Vm.shape
         s = assemble_phie(self.nodes, self._elems_np, c.sigma_il.contiguous(), c.sigma_it.contiguous(),
                           c.sigma_el.contiguous(), c.sigma_et.contiguous(), self.fibres.contiguous())
@@ -291,6 +333,7 @@ class Monodomain:
             if verbose:
                 print(phi.min().item(), phi.max().item(), int(buf["step_iters"][k + 1].item()), flush=True)
         check(lib.tcb_mono_check(C.byref(m), stream_ptr()))
+        out = self._to_caller(out)
         self.phi_e = out
         self.phie_iters = buf["step_iters"][1:].cpu()
         if self.result_path is not None:
