@@ -155,7 +155,8 @@ typedef struct tcb_mono {
     float* p2;               /* batch solver only: second search-direction buffer, n_pad */
     float* at;
     float* rt;
-    float* snapshots;        /* row j = solution of step j*per_frame, n_nodes per row; may be NULL */
+    float* snapshots;        /* row j = solution of step j*per_frame, n_nodes per row; may be NULL;
+                                with snap_ring > 0 a ring of snap_ring rows: frame j goes to row j % snap_ring */
     /* stimuli and schedule */
     const uint32_t* stim_bits;   /* per node: bit s set if the node is in stimulus s */
     const float* step_t;         /* [nt+1]: fp32 of the accumulated time t_n */
@@ -166,6 +167,8 @@ typedef struct tcb_mono {
     int32_t max_iter, linear_guess, at_rt, per_frame;
     int32_t a_split;         /* 1 if every a_val == fp32(fp32(m_val*cm) + k_val) (tcb_assemble_system's check) */
     float cm, dt;
+    int32_t snap_ring;       /* 0: snapshots holds every frame; > 0: rows in the snapshot ring (the
+                                caller copies each frame out before it is overwritten) */
     /* device bookkeeping (caller-allocated, zero-initialised) */
     int32_t* step_iters;     /* [nt+1] CG iterations of each step */
     int32_t* counter;        /* [4]: next step, error code, 2 spare */

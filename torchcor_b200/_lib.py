@@ -44,7 +44,7 @@ class tcb_mono(C.Structure):
         ("stim_bits", _vp), ("step_t", _vp), ("step_stim", _vp), ("stim_amp", C.c_float * TCB_MAX_STIMULI),
         ("a_tol", _f64), ("r_tol", _f64),
         ("max_iter", _i32), ("linear_guess", _i32), ("at_rt", _i32), ("per_frame", _i32), ("a_split", _i32),
-        ("cm", C.c_float), ("dt", C.c_float),
+        ("cm", C.c_float), ("dt", C.c_float), ("snap_ring", _i32),
         ("step_iters", _vp), ("counter", _vp), ("scratch", _vp), ("barrier", _vp),
         ("params", _vp),
     ]

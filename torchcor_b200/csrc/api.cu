@@ -51,6 +51,8 @@ MonoDev make_dev(const tcb_mono* m) {
     d.at = m->at;
     d.rt = m->rt;
     d.snap = m->snapshots;
+    d.snap_ring = m->snap_ring;
+    d.pad = 0;
     d.stim_bits = m->stim_bits;
     d.step_t = m->step_t;
     d.step_stim = m->step_stim;
@@ -83,7 +85,8 @@ int validate(const tcb_mono* m) {
         !m->step_stim || !m->step_iters || !m->counter || !m->scratch || !m->barrier || !m->params)
         return fail(TCB_EINVAL, "tcb_mono: null pointer");
     if (m->model != TCB_MODEL_MS && !m->tables) return fail(TCB_EINVAL, "tcb_mono: null tables");
-    if (m->max_iter < 0 || m->per_frame < 0) return fail(TCB_EINVAL, "tcb_mono: negative max_iter/per_frame");
+    if (m->max_iter < 0 || m->per_frame < 0 || m->snap_ring < 0)
+        return fail(TCB_EINVAL, "tcb_mono: negative max_iter/per_frame/snap_ring");
     return TCB_OK;
 }
 }  // namespace

@@ -147,7 +147,8 @@ __global__ void mono_finish_kernel(MonoDev d) {
     if (last < 1) return;
     const float* u = d.x + ring_cur(n) * d.n_pad;
     const float t = d.step_t[last];
-    float* snap = (d.snap && d.per_frame > 0 && last % d.per_frame == 0) ? d.snap + (last / d.per_frame) * d.n : nullptr;
+    float* snap = (d.snap && d.per_frame > 0 && last % d.per_frame == 0) ? d.snap + snap_row(d, last / d.per_frame) * d.n
+                                                                          : nullptr;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += (int64_t)gridDim.x * blockDim.x) {
         float v = u[i];
         if (d.at_rt) at_rt_update(v, t, d.at, d.rt, i);

@@ -33,7 +33,8 @@ __device__ __forceinline__ StepView step_view(const MonoDev& d, int64_t n) {
     v.t_prev = d.step_t[prev];
     // step numbers and frame intervals are below 2^31 (validated on the host)
     const uint32_t pv = (uint32_t)prev, pf = (uint32_t)d.per_frame;
-    v.snap = (d.snap && d.per_frame > 0 && prev >= 1 && pv % pf == 0u) ? d.snap + (int64_t)(pv / pf) * d.n : nullptr;
+    v.snap = (d.snap && d.per_frame > 0 && prev >= 1 && pv % pf == 0u) ? d.snap + snap_row(d, pv / pf) * d.n
+                                                                      : nullptr;
     v.smask = d.step_stim[n];
     return v;
 }

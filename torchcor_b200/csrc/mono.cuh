@@ -26,10 +26,14 @@ struct MonoDev {
     int32_t max_iter, linear_guess, at_rt, per_frame;
     int32_t a_split;   // A == fp32(fp32(M*Cm) + K') verified at assembly
     float cm, dt;
+    int32_t snap_ring, pad;   // snapshot rows: 0 = one per frame, > 0 = ring of that many
     float amp[TCB_MAX_STIMULI];
 };
 
 MonoDev make_dev(const tcb_mono* m);
+
+// snapshot row of frame f (frame f = solution of step f * per_frame)
+__host__ __device__ inline int64_t snap_row(const MonoDev& d, int64_t f) { return d.snap_ring > 0 ? f % d.snap_ring : f; }
 
 // membrane-potential ring: step n reads slot (n-1)%3, guesses from (n+1)%3, writes n%3
 __host__ __device__ inline int64_t ring_cur(int64_t n) { return (n + 2) % 3; }

@@ -101,7 +101,9 @@ class Monodomain:
 
     def _to_caller(self, t):
         """Per-node tensor (last axis) from the internal numbering to the caller's."""
-        return t if t is None or self._inv_t is None else t[..., self._inv_t]
+        if t is None or self._inv_t is None:
+            return t
+        return t[..., self._inv_t if t.device == self._inv_t.device else self._inv_t.cpu()]
 
     def _to_internal(self, t):
         return t if t is None or self._perm_t is None else t[..., self._perm_t]
@@ -126,7 +128,8 @@ class Monodomain:
         return s
 
     # -------------------------------------------------------------- time loop
-    def _setup(self, a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep_snapshots):
+    def _setup(self, a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep_snapshots,
+               snapshot_ring=0):
         s = self.system
         dev = self.device
         im = self.ionic_model
@@ -140,15 +143,21 @@ class Monodomain:
         if per_frame == 0:
             raise ZeroDivisionError("snapshot_interval is shorter than dt")
         n_snap = nt // per_frame + 1
-        snaps = torch.empty((n_snap, n), **f32) if keep_snapshots else None
-        if snaps is not None:
+        ring = int(snapshot_ring) if keep_snapshots and snapshot_ring else 0
+        snaps = torch.empty((ring if ring else n_snap, n), **f32) if keep_snapshots else None
+        host_snaps = None
+        if ring:
+            # frames stream to pinned host memory; frame 0 is the initial state
+            host_snaps = torch.empty((n_snap, n), dtype=torch.float32, pin_memory=True)
+            host_snaps[0].copy_(u0)
+        elif snaps is not None:
             snaps[0] = u0
         t32, mask = self.stimuli.schedule(nt, self.dt)
         sim = dict(
             x=x, bp=torch.zeros(n_pad, **f32), r=torch.zeros(n_pad, **f32), p=torch.zeros(n_pad, **f32),
             ap=torch.zeros(n_pad, **f32), z=torch.zeros(n_pad, **f32), p2=torch.zeros(n_pad, **f32),
             at=torch.full((n,), -1.0, **f32), rt=torch.full((n,), -1.0, **f32),
-            snaps=snaps, u0=u0,
+            snaps=snaps, u0=u0, ring=ring, host_snaps=host_snaps,
             stim_bits=torch.from_numpy(self._stim_bits().view(np.int32)).to(dev),
             step_t=torch.from_numpy(t32).to(dev), step_stim=torch.from_numpy(mask.view(np.int32)).to(dev),
             step_iters=torch.zeros(nt + 1, device=dev, dtype=torch.int32),
@@ -172,6 +181,7 @@ class Monodomain:
         m.a_tol, m.r_tol, m.max_iter = float(a_tol), float(r_tol), int(max_iter)
         m.linear_guess, m.at_rt, m.per_frame = int(bool(linear_guess)), int(bool(calculate_AT_RT)), per_frame
         m.cm, m.dt = float(self.Cm), float(self.dt)
+        m.snap_ring = ring
         m.a_split = int(s.a_split)
         m.step_iters, m.counter = ptr(sim["step_iters"]), ptr(sim["counter"])
         m.scratch, m.barrier = ptr(sim["scratch"]), ptr(sim["barrier"])
@@ -244,18 +254,79 @@ class Monodomain:
         el = time.time() - t0
         return self.current_solution().clone(), int(sim["step_iters"][n].item()), 0.0, el
 
+    # -------------------------------------------------- streamed snapshot output
+    def _snapshot_stream_init(self):
+        sim = self._sim
+        sim["copy_stream"] = torch.cuda.Stream(self.device)
+        sim["copied"] = [None] * sim["ring"]     # event per ring row: its last copy to the host is done
+        sim["next_frame"] = 1                    # next frame to copy out (frame 0 is the initial state)
+
+    def _frames_written(self):
+        """Frames whose snapshot rows the steps launched so far have written (the
+        ionic kernel of step f*per_frame + 1 writes frame f)."""
+        sim = self._sim
+        return (sim["next_step"] - 2) // sim["per_frame"] if sim["next_step"] >= 2 else 0
+
+    def _before_steps(self, first_step, n_steps):
+        """Make the compute stream wait until the ring rows that steps
+        [first_step, first_step + n_steps) will overwrite have been copied out."""
+        sim = self._sim
+        pf, R = sim["per_frame"], sim["ring"]
+        cur = torch.cuda.current_stream(self.device)
+        f0 = max(1, (first_step - 1 + pf - 1) // pf)
+        f1 = (first_step + n_steps - 2) // pf
+        for f in range(max(f0, f1 - R + 1), f1 + 1):
+            ev = sim["copied"][f % R]
+            if ev is not None:
+                cur.wait_event(ev)
+
+    def _drain_snapshots(self, final=False):
+        """Queue the copies of every frame written so far (on the copy stream, after
+        the compute stream's work); with ``final`` also the last step's frame, which
+        the finish kernel writes, and wait for all copies."""
+        sim = self._sim
+        pf, R = sim["per_frame"], sim["ring"]
+        last = self.nt // pf if final else self._frames_written()
+        if sim["next_frame"] > last:
+            if final:
+                sim["copy_stream"].synchronize()
+            return
+        cur = torch.cuda.current_stream(self.device)
+        done = torch.cuda.Event()
+        done.record(cur)
+        cs = sim["copy_stream"]
+        cs.wait_event(done)
+        with torch.cuda.stream(cs):
+            for f in range(sim["next_frame"], last + 1):
+                sim["host_snaps"][f].copy_(sim["snaps"][f % R], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(cs)
+                sim["copied"][f % R] = ev
+        sim["next_frame"] = last + 1
+        if final:
+            cs.synchronize()
+
     def finish(self, result_path=None, calculate_AT_RT=True):
         """AT/RT update and snapshot of the last step, error check, result files
         (the tail of monodomain.py:141-226).  Returns the total CG iterations."""
         sim = self._sim
         st = sim["struct"]
         lib = _lib.load()
+        if sim.get("ring") and self.nt % sim["per_frame"] == 0:
+            self._drain_snapshots()
+            ev = sim["copied"][(self.nt // sim["per_frame"]) % sim["ring"]]
+            if ev is not None:
+                torch.cuda.current_stream(self.device).wait_event(ev)
         check(lib.tcb_mono_finish(C.byref(st), stream_ptr()))
         check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
         self.n_total_iter = int(sim["step_iters"].sum().item())
         self.activation_time = self._to_caller(sim["at"])
         self.repolarization_time = self._to_caller(sim["rt"])
-        self.solutions = self._to_caller(sim["snaps"])
+        if sim.get("ring"):
+            self._drain_snapshots(final=True)
+            self.solutions = self._to_caller(sim["host_snaps"])
+        else:
+            self.solutions = self._to_caller(sim["snaps"])
         if result_path is not None:
             rp = Path(result_path)
             rp.mkdir(parents=True, exist_ok=True)
@@ -348,17 +419,33 @@ class Monodomain:
                            snapshot_interval < self.T)
 
     def solve(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1,
-              verbose=True, result_path=None):
+              verbose=True, result_path=None, snapshot_ring=None):
+        """monodomain.py:141-226.  ``snapshot_ring=R`` keeps only R snapshot frames on
+        the device and streams every frame, as soon as it is written, into a pinned host
+        tensor on a separate stream (``solutions`` is then that host tensor); the
+        default keeps every frame on the device, as the reference does."""
         self.result_path = Path(result_path) if result_path is not None else None
         if self.result_path is not None:
             self.result_path.mkdir(parents=True, exist_ok=True)
         self.assemble()
         keep = snapshot_interval < self.T
-        sim = self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep)
+        if snapshot_ring is not None and int(snapshot_ring) < 1:
+            raise ValueError("snapshot_ring must be a positive number of frames")
+        sim = self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep,
+                          snapshot_ring or 0)
         t0 = time.time()
-        chunk = max(1, sim["per_frame"]) * (1 if verbose and snapshot_interval != self.T else 1000)
+        ring = sim["ring"]
+        if ring:
+            self._snapshot_stream_init()
+            chunk = max(1, sim["per_frame"])
+        else:
+            chunk = max(1, sim["per_frame"]) * (1 if verbose and snapshot_interval != self.T else 1000)
         while sim["next_step"] <= self.nt:
+            if ring:
+                self._before_steps(sim["next_step"], min(chunk, self.nt + 1 - sim["next_step"]))
             self.run_steps(chunk)
+            if ring:
+                self._drain_snapshots()
             if verbose and snapshot_interval != self.T:
                 torch.cuda.synchronize(self.device)
                 done = sim["next_step"] - 1
