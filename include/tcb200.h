@@ -65,6 +65,28 @@ int tcb_pattern_build(const int32_t* elems, int64_t n_elems, int32_t k, int64_t 
  * (each slice holds 32 * its widest row entries).  Host code. */
 int tcb_sell_layout(const int32_t* rowptr, int64_t n_rows, int64_t* slice_ptr, int64_t* n_entries);
 
+/* ---------------------------------------------------------------- device ingest
+ * Mesh ingest on the device (replaces MeshReader's np.loadtxt, mesh.py:26-63, and
+ * the COO build + coalesce of assemble.py:217-248 for device-resident elements).
+ * Text: tcb_text_scratch(n) int64 words of scratch; tcb_text_newlines gives the
+ * newline count (pos == NULL) or positions; tcb_text_parse parses `rows` lines from
+ * line `first_line` (0-based), skipping `skip` fields and reading `cols` fields as
+ * int64 (as_int) or correctly rounded float64 into out[rows][cols]; rows it cannot
+ * parse exactly are counted in *bad (device int64, caller-zeroed).
+ * Pattern: tcb_pattern_device with work = 2*(N+1) int64, keys = k*k*E uint64,
+ * iwork = 2*N+1 int32 returns nnz; tcb_pattern_device_emit writes the same arrays
+ * as tcb_pattern_build (device pointers). */
+int64_t tcb_text_scratch(int64_t n_bytes);
+int tcb_text_newlines(const char* text, int64_t n_bytes, int64_t* scratch, int64_t* pos, int64_t cap, int64_t* count,
+                      void* stream);
+int tcb_text_parse(const char* text, int64_t n_bytes, const int64_t* newlines, int64_t n_newlines, int64_t first_line,
+                   int64_t rows, int32_t skip, int32_t cols, int32_t as_int, void* out, int64_t* bad, void* stream);
+int tcb_pattern_device(const int32_t* elems, int64_t n_elems, int32_t k, int64_t n_nodes, int64_t* work,
+                       uint64_t* keys, int32_t* iwork, int64_t* nnz, void* stream);
+int tcb_pattern_device_emit(const int64_t* work, const uint64_t* keys, int64_t n_elems, int32_t k, int64_t n_nodes,
+                            int32_t* rowptr, int32_t* col, int32_t* slot_ptr, int32_t* slot_src, int32_t* diag,
+                            void* stream);
+
 /* ---------------------------------------------------------------- assembly
  * Element matrices of P1 tetrahedra (k=4) or surface triangles (k=3).
  * Replaces Matrices3D.construct_local_matrices (assemble.py:202-215) and

@@ -69,6 +69,11 @@ SIGNATURES = [
     ("tcb_last_error", C.c_int, [C.c_char_p, _i64]),
     ("tcb_pattern_size", C.c_int, [_vp, _i64, _i32, _i64, _pi64]),
     ("tcb_pattern_build", C.c_int, [_vp, _i64, _i32, _i64, _vp, _vp, _vp, _vp, _vp]),
+    ("tcb_text_scratch", _i64, [_i64]),
+    ("tcb_text_newlines", C.c_int, [_vp, _i64, _vp, _vp, _i64, _pi64, _vp]),
+    ("tcb_text_parse", C.c_int, [_vp, _i64, _vp, _i64, _i64, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
+    ("tcb_pattern_device", C.c_int, [_vp, _i64, _i32, _i64, _vp, _vp, _vp, _pi64, _vp]),
+    ("tcb_pattern_device_emit", C.c_int, [_vp, _vp, _i64, _i32, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("tcb_sell_layout", C.c_int, [_vp, _i64, _vp, _pi64]),
     ("tcb_assemble_local", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("tcb_assemble_gather", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),

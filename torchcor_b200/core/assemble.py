@@ -26,22 +26,36 @@ def n_padded(n):
 
 @dataclass
 class Pattern:
+    """CSR pattern and scatter map: numpy arrays (host build) or device tensors."""
     n_nodes: int
     k: int
-    rowptr: np.ndarray
-    col: np.ndarray
-    slot_ptr: np.ndarray
-    slot_src: np.ndarray
-    diag: np.ndarray
+    rowptr: object
+    col: object
+    slot_ptr: object
+    slot_src: object
+    diag: object
+    n_nonzero: int = None
 
     @property
     def nnz(self):
-        return int(self.rowptr[-1])
+        return int(self.rowptr[-1]) if self.n_nonzero is None else self.n_nonzero
+
+    def on(self, name, device):
+        """One of the arrays as a device tensor."""
+        a = getattr(self, name)
+        return a if isinstance(a, torch.Tensor) else torch.from_numpy(a).to(device)
+
+    def host(self, name):
+        a = getattr(self, name)
+        return a.cpu().numpy() if isinstance(a, torch.Tensor) else a
 
 
-def build_pattern(elems: np.ndarray, n_nodes: int) -> Pattern:
+def build_pattern(elems, n_nodes: int) -> Pattern:
     """CSR pattern (equal to the reference's coalesce -> to_sparse_csr) and the
-    contribution map in the reference's COO order (host C++)."""
+    contribution map in the reference's COO order: host C++ for a numpy array,
+    the device build (same arrays, bit for bit) for a CUDA tensor."""
+    if isinstance(elems, torch.Tensor):
+        return build_pattern_device(elems, n_nodes)
     lib = _lib.load()
     el = np.ascontiguousarray(elems, dtype=np.int32)
     E, k = el.shape
@@ -55,6 +69,33 @@ def build_pattern(elems: np.ndarray, n_nodes: int) -> Pattern:
     check(lib.tcb_pattern_build(ptr(el), E, k, n_nodes, ptr(rowptr), ptr(col), ptr(slot_ptr), ptr(slot_src),
                                 ptr(diag)))
     return Pattern(n_nodes, k, rowptr, col, slot_ptr, slot_src, diag)
+
+
+def build_pattern_device(elems: torch.Tensor, n_nodes: int) -> Pattern:
+    """``build_pattern`` on the GPU for device-resident elements."""
+    lib = _lib.load()
+    dev = elems.device
+    el = elems.to(torch.int32).contiguous()
+    E, k = el.shape
+    work = torch.empty(2 * (n_nodes + 1), device=dev, dtype=torch.int64)
+    keys = torch.empty(k * k * E, device=dev, dtype=torch.int64)     # uint64 keys
+    iwork = torch.empty(2 * n_nodes + 1, device=dev, dtype=torch.int32)
+    nnz = C.c_int64()
+    s = stream_ptr()
+    check(lib.tcb_pattern_device(ptr(el), E, k, n_nodes, ptr(work), ptr(keys), ptr(iwork), C.byref(nnz), s))
+    i32 = dict(device=dev, dtype=torch.int32)
+    rowptr, col = torch.empty(n_nodes + 1, **i32), torch.empty(nnz.value, **i32)
+    slot_ptr, slot_src = torch.empty(nnz.value + 1, **i32), torch.empty(k * k * E, **i32)
+    diag = torch.empty(n_nodes, **i32)
+    check(lib.tcb_pattern_device_emit(ptr(work), ptr(keys), E, k, n_nodes, ptr(rowptr), ptr(col), ptr(slot_ptr),
+                                      ptr(slot_src), ptr(diag), s))
+    return Pattern(n_nodes, k, rowptr, col, slot_ptr, slot_src, diag, n_nonzero=nnz.value)
+
+
+def _elems_on(elems, dev):
+    if isinstance(elems, torch.Tensor):
+        return elems.to(device=dev, dtype=torch.int32).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(elems, dtype=np.int32)).to(dev)
 
 
 def local_matrices(nodes, elems, sl, st, fibres):
@@ -103,16 +144,16 @@ def assemble_system(nodes, elems_np, sl, st, fibres, dt, chi=140, cm=0.01, theta
     pat = pattern if pattern is not None else build_pattern(elems_np, n)
     nnz = pat.nnz
     k = pat.k
-    elems = torch.from_numpy(np.ascontiguousarray(elems_np, dtype=np.int32)).to(dev)
+    elems = _elems_on(elems_np, dev)
     ke, mw = local_matrices(nodes, elems, sl, st, fibres)
-    slot_ptr = torch.from_numpy(pat.slot_ptr).to(dev)
-    slot_src = torch.from_numpy(pat.slot_src).to(dev)
+    slot_ptr = pat.on("slot_ptr", dev)
+    slot_src = pat.on("slot_src", dev)
     k_val = torch.empty(nnz, device=dev, dtype=torch.float32)
     m_val = torch.empty(nnz, device=dev, dtype=torch.float32)
     s = stream_ptr()
     check(lib.tcb_assemble_gather(k, ptr(slot_ptr), ptr(slot_src), nnz, ptr(ke), ptr(mw), ptr(k_val), ptr(m_val), s))
     del ke, mw, slot_ptr, slot_src
-    diag = torch.from_numpy(pat.diag).to(dev)
+    diag = pat.on("diag", dev)
     a_val = torch.empty(nnz, device=dev, dtype=torch.float32)
     krhs = torch.empty(nnz, device=dev, dtype=torch.float32)
     d_inv = torch.empty(n_pad, device=dev, dtype=torch.float32)
@@ -123,9 +164,10 @@ def assemble_system(nodes, elems_np, sl, st, fibres, dt, chi=140, cm=0.01, theta
     n_slices = (n + _lib.TCB_SLICE - 1) // _lib.TCB_SLICE
     sp = np.empty(n_slices + 1, dtype=np.int64)
     n_entries = C.c_int64()
-    check(lib.tcb_sell_layout(ptr(pat.rowptr), n, ptr(sp), C.byref(n_entries)))
-    rowptr = torch.from_numpy(pat.rowptr).to(dev)
-    col = torch.from_numpy(pat.col).to(dev)
+    rowptr_host = pat.host("rowptr")           # keep the host copy alive across the call
+    check(lib.tcb_sell_layout(ptr(rowptr_host), n, ptr(sp), C.byref(n_entries)))
+    rowptr = pat.on("rowptr", dev)
+    col = pat.on("col", dev)
     slice_ptr = torch.from_numpy(sp).to(dev)
     ne = n_entries.value
     sell_col = torch.empty(ne, device=dev, dtype=torch.int32)
@@ -156,9 +198,9 @@ def assemble_phie(nodes, elems_np, sl_i, st_i, sl_e, st_e, fibres) -> System:
     n_pad = n_padded(n)
     pat = build_pattern(elems_np, n)
     nnz, k = pat.nnz, pat.k
-    elems = torch.from_numpy(np.ascontiguousarray(elems_np, dtype=np.int32)).to(dev)
-    slot_ptr = torch.from_numpy(pat.slot_ptr).to(dev)
-    slot_src = torch.from_numpy(pat.slot_src).to(dev)
+    elems = _elems_on(elems_np, dev)
+    slot_ptr = pat.on("slot_ptr", dev)
+    slot_src = pat.on("slot_src", dev)
     s = stream_ptr()
 
     def stiffness(sl, st):
@@ -170,7 +212,7 @@ def assemble_phie(nodes, elems_np, sl_i, st_i, sl_e, st_e, fibres) -> System:
 
     kie, mass = stiffness(sl_i + sl_e, st_i + st_e)
     ki, _ = stiffness(sl_i, st_i)
-    diag = torch.from_numpy(pat.diag).to(dev)
+    diag = pat.on("diag", dev)
     a_val = torch.empty(nnz, device=dev, dtype=torch.float32)
     zero = torch.empty(nnz, device=dev, dtype=torch.float32)
     d_inv = torch.empty(n_pad, device=dev, dtype=torch.float32)
@@ -179,9 +221,10 @@ def assemble_phie(nodes, elems_np, sl_i, st_i, sl_e, st_e, fibres) -> System:
     n_slices = (n + _lib.TCB_SLICE - 1) // _lib.TCB_SLICE
     sp = np.empty(n_slices + 1, dtype=np.int64)
     n_entries = C.c_int64()
-    check(lib.tcb_sell_layout(ptr(pat.rowptr), n, ptr(sp), C.byref(n_entries)))
-    rowptr = torch.from_numpy(pat.rowptr).to(dev)
-    col = torch.from_numpy(pat.col).to(dev)
+    rowptr_host = pat.host("rowptr")           # keep the host copy alive across the call
+    check(lib.tcb_sell_layout(ptr(rowptr_host), n, ptr(sp), C.byref(n_entries)))
+    rowptr = pat.on("rowptr", dev)
+    col = pat.on("col", dev)
     slice_ptr = torch.from_numpy(sp).to(dev)
     ne = n_entries.value
     sell_col = torch.empty(ne, device=dev, dtype=torch.int32)

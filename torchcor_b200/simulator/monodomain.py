@@ -73,10 +73,36 @@ class Monodomain:
         self._perm_t = self._inv_t = None
 
     # ------------------------------------------------------------------ input
-    def load_mesh(self, path="Data/ventricle/Case_1", unit_conversion=1000):
+    def load_mesh(self, path="Data/ventricle/Case_1", unit_conversion=1000, device_ingest=True):
+        """Read the openCARP mesh in ``path`` (monodomain.py:60-73).  With
+        ``device_ingest`` (default) the files are parsed and the CSR pattern is built
+        on the GPU (same arrays as the host reader and pattern builder); files the
+        device parser cannot read exactly go through the host reader, listed in
+        ``self.ingest_host_files``."""
         self.mesh_path = Path(path)
+        if device_ingest and not self.reorder:
+            from torchcor_b200.core.ingest import read_mesh_device
+            nodes, elems, regions, fibres, on_host = read_mesh_device(path, self.device, unit_conversion)
+            self.ingest_host_files = on_host
+            self.load_device_arrays(nodes, elems, regions, fibres)
+            return
         nodes, elems, regions, fibres = MeshReader(path).read(unit_conversion=unit_conversion)
+        self.ingest_host_files = None
         self.load_arrays(nodes, elems, regions, fibres)
+
+    def load_device_arrays(self, nodes, elems, regions, fibres):
+        """Mesh already on the device (tensors): nodes (N,3) in mm, elems (E,3|4),
+        per-element regions and fibres.  The pattern of the assembly is then built
+        on the device too."""
+        dev = self.device
+        self.n_nodes = int(nodes.shape[0])
+        self.nodes = nodes.to(device=dev, dtype=torch.float32).contiguous()
+        self.elems = elems.to(device=dev, dtype=torch.int32).contiguous()
+        self._elems_np = self.elems                    # device elements: device pattern build
+        self.regions = regions.to(device=dev, dtype=torch.int).contiguous()
+        self.fibres = fibres.to(device=dev, dtype=torch.float32).contiguous()
+        self.stimuli = Stimuli(self.n_nodes, dev, self.dtype)
+        self.conductivity = Conductivity(self.regions, dtype=self.dtype)
 
     def load_arrays(self, nodes, elems, regions, fibres):
         """Mesh already in memory: nodes (N,3) in mm, elems (E,3|4), per-element regions and fibres."""
