@@ -38,6 +38,8 @@ sys.path.insert(0, str(ROOT))
 import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
+from torchcor_b200 import replicas  # noqa: E402
+
 METRIC = "node-steps/s"
 
 
@@ -225,12 +227,7 @@ def tcb_arm(a, wl, world, rank, local):
         sim.run_steps(a.steps)
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        torch.distributed.barrier()
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.reduce_max(e0.elapsed_time(e1))     # slowest rank (replicas only)
     _lib.check(lib.tcb_mono_check(C.byref(st), stream.cuda_stream))
     t0s = a.warmup + a.profile_steps
     iters = sim._sim["step_iters"][t0s + 1: t0s + a.steps + 1].sum().item()
@@ -272,10 +269,7 @@ def tcb_arm(a, wl, world, rank, local):
                    wl.n_nodes * 4 + (wl.nt + 1) * 8)
             d2h = 2 * wl.n_nodes * 4 + (wl.nt // int(1.0 / wl.dt) + 1) * wl.n_nodes * 4 + (wl.nt + 1) * 4
             del sim2
-        if world > 1:
-            t = torch.tensor([wall], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = replicas.reduce_max(wall)
         e2e = {"value": world * wl.n_nodes * wl.nt / wall, "unit": METRIC,
                "h2d_bytes_per_step": int(h2d // wl.nt), "d2h_bytes_per_step": int(d2h // wl.nt),
                "what": f"one Monodomain.solve of the workload (T={wl.T} ms, {wl.nt} steps) from host arrays: "
@@ -347,6 +341,8 @@ def batch_arm(a, world, rank, local):
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     K = a.steps if not replay else (a.steps // G) * G
+    if world > 1:
+        torch.distributed.barrier()
     with ClockSampler(local) as clk:
         e0.record(stream)
         if replay:
@@ -356,7 +352,7 @@ def batch_arm(a, world, rank, local):
             batch.step(K)
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1)
+    ms = replicas.reduce_max(e0.elapsed_time(e1))     # slowest rank (each rank runs the batch)
     batch.check()
     iters = sum(int(s._sim["step_iters"].sum().item()) for s in batch.sims)
     # CG passes of the timed steps: the batch kernel runs max_i(it_i + 1) passes a
@@ -390,7 +386,8 @@ def batch_arm(a, world, rank, local):
             torch.cuda.synchronize(dev)
             plain_ms += e0.elapsed_time(e1)
             del sim
-    plain = total * K / (plain_ms / 1e3) if plain_ms else None
+    plain_ms = replicas.reduce_max(plain_ms)
+    plain = world * total * K / (plain_ms / 1e3) if plain_ms else None
     if rank != 0:
         return
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": a.warmup,
@@ -423,11 +420,16 @@ def serving_arm(a, world, rank, local):
     torch.cuda.set_device(dev)
     reqs = serving.generate_requests(count=a.requests, seed=2025 + rank, capacity=a.capacity, load=a.load)
     server = serving.Server(dev)
+    if world > 1:
+        torch.distributed.barrier()
     with ClockSampler(local) as clk:
         summ = server.run(reqs)
+    # each rank serves its own stream: whole-job rate = all ranks' node-steps / slowest wall
+    total_ns = replicas.reduce_sum(summ["node_steps"])
+    wall = replicas.reduce_max(summ["wall_s"])
     if rank != 0:
         return
-    line = {"metric": METRIC, "value": summ["node_steps_per_s"] * world, "unit": METRIC, "n_gpus": world,
+    line = {"metric": METRIC, "value": total_ns / wall, "unit": METRIC, "n_gpus": world,
             "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"serving: {a.requests} requests, Poisson arrivals offered at {a.load} x "
