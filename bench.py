@@ -219,14 +219,25 @@ def tcb_arm(a, wl, world, rank, local):
     p_iters = sim._sim["step_iters"][s0: s0 + a.profile_steps].sum().item()
     kp = p_iters / a.profile_steps + 1.0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the timed steps replay CUDA graphs of G steps (Monodomain.capture_steps), the
+    # remainder runs as plain launches
+    G = a.graph_steps if a.graph_steps > 0 else 0
+    replay = sim.capture_steps(G) if G and a.steps >= G else None
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
         e0.record(stream)
-        sim.run_steps(a.steps)
+        done = 0
+        if replay:
+            for _ in range(a.steps // G):
+                replay()
+            done = (a.steps // G) * G
+        if a.steps > done:
+            sim.run_steps(a.steps - done)
         e1.record(stream)
         torch.cuda.synchronize(dev)
+    del replay
     ms = replicas.reduce_max(e0.elapsed_time(e1))     # slowest rank (replicas only)
     _lib.check(lib.tcb_mono_check(C.byref(st), stream.cuda_stream))
     t0s = a.warmup + a.profile_steps
@@ -289,7 +300,7 @@ def tcb_arm(a, wl, world, rank, local):
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": wl.name, "nodes": wl.n_nodes, "elements": int(len(wl.elems)), "nnz": sys_.nnz,
                    "dt_ms": wl.dt, "T_ms": wl.T, "parallelism": "replicas only" if world > 1 else "single",
-                   "cg_tol": 1e-5, "cg_iterations_per_step": iters / a.steps,
+                   "cg_tol": 1e-5, "cg_iterations_per_step": iters / a.steps, "cuda_graph_steps": G,
                    "l2": "inputs larger than L2 (per-step working set > 300 MB)",
                    "simulated_ms_per_s": world * wl.dt * a.steps / (ms / 1e3)},
         "gpu_launches": 2 * a.steps,
@@ -449,8 +460,11 @@ def main():
     ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube", "batch_cubes", "serving"])
     ap.add_argument("--requests", type=int, default=512, help="serving mode: requests in the stream")
     ap.add_argument("--load", type=float, default=0.9, help="serving mode: offered load / capacity")
-    ap.add_argument("--capacity", type=float, default=5e9, help="serving mode: node-steps/s the rate assumes")
-    ap.add_argument("--graph-steps", type=int, default=0, help="batch mode: steps per captured CUDA graph")
+    ap.add_argument("--capacity", type=float, default=3.5e9,
+                    help="serving mode: node-steps/s the arrival rate assumes (measured for this mix)")
+    ap.add_argument("--graph-steps", type=int, default=-1,
+                    help="steps per captured CUDA graph in the timed region (0 = plain launches; "
+                         "default 100 for a single simulation, 0 for a batch)")
     ap.add_argument("--no-plain", action="store_true", help="batch mode: skip the one-at-a-time comparison")
     ap.add_argument("--cg-variant", type=int, default=0, choices=[0, 1, 2, 3],
                     help="batch mode: batched CG variant (1/2 streaming, 3 staged); 0 = autotuned")
@@ -460,6 +474,8 @@ def main():
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be at least 3")
+    if a.graph_steps < 0:
+        a.graph_steps = 0 if a.workload == "batch_cubes" else 100
     from torchcor_b200.workloads import WORKLOADS
     world, rank, local = dist_setup(a.impl)
     if a.workload == "serving":
