@@ -464,7 +464,7 @@ def main():
                     help="serving mode: node-steps/s the arrival rate assumes (measured for this mix)")
     ap.add_argument("--graph-steps", type=int, default=-1,
                     help="steps per captured CUDA graph in the timed region (0 = plain launches; "
-                         "default 100 for a single simulation, 0 for a batch)")
+                         "default 100 for a single simulation, 50 for a batch)")
     ap.add_argument("--no-plain", action="store_true", help="batch mode: skip the one-at-a-time comparison")
     ap.add_argument("--cg-variant", type=int, default=0, choices=[0, 1, 2, 3],
                     help="batch mode: batched CG variant (1/2 streaming, 3 staged); 0 = autotuned")
@@ -475,7 +475,7 @@ def main():
     if a.warmup < 3:
         ap.error("--warmup must be at least 3")
     if a.graph_steps < 0:
-        a.graph_steps = 0 if a.workload == "batch_cubes" else 100
+        a.graph_steps = 50 if a.workload == "batch_cubes" else 100
     from torchcor_b200.workloads import WORKLOADS
     world, rank, local = dist_setup(a.impl)
     if a.workload == "serving":

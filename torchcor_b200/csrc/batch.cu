@@ -246,16 +246,11 @@ extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* st
         return fail(TCB_EINVAL, "tcb_batch_run: plan CG grid out of range");
     cudaStream_t s = as_stream(stream);
     const BatchWS* W = static_cast<const BatchWS*>(plan->workspace);
-    BatchWS hv;
-    memset(&hv, 0, sizeof hv);
-    for (int g = 0; g < kBatchGroups; ++g) hv.groups[g].model = plan->group_model[g];
     for (int64_t k = 0; k < steps; ++k) {
-        for (int g = 0; g < plan->n_groups; ++g) {
-            int st = launch_batch_ionic(W, hv, g, plan->group_tiles[g],
-                                        plan->group_shared[g] ? plan->group_consts[g] : nullptr, s);
-            if (st) return st;
-        }
-        int st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_variant, plan->cg_stage_bytes, s);
+        int st = launch_batch_ionic_all(W, plan->n_groups, plan->group_model, plan->group_tiles, plan->group_shared,
+                                        plan->group_consts, s);
+        if (st) return st;
+        st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_variant, plan->cg_stage_bytes, s);
         if (st) return st;
     }
     return TCB_OK;

@@ -54,8 +54,8 @@ struct BatchWS {
     BatchGroup groups[kBatchGroups];
 };
 
-int launch_batch_ionic(const BatchWS* ws_dev, const BatchWS& ws_host_view, int g, int64_t total_tiles,
-                       const void* shared_consts_host, cudaStream_t s);
+int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* models, const int64_t* tiles,
+                           const int32_t* shared, const char (*consts)[1024], cudaStream_t s);
 // batched CG variants: 1 / 2 = streaming, sized for 1 / 2 blocks per SM;
 // 3 = ELL streams staged in shared memory by bulk copies, 1 block per SM
 int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int stage_bytes, cudaStream_t s);

@@ -1,5 +1,5 @@
-// Batched ionic step: one launch per ionic model covers every simulation of
-// that model in the batch (compiled with -fmad=false, like ionic.cu; the
+// Batched ionic step: one launch covers every simulation of the batch, each
+// block running the model of its group (compiled with -fmad=false, like ionic.cu; the
 // per-node work is the same ionic_node the single-simulation kernel runs).
 //
 // Threads walk a virtual node space made of each simulation's 128-node tiles;
@@ -24,25 +24,18 @@ constexpr int kThreads = kBatchTile;   // a block walks 128-node tiles
 constexpr int kMaxTilesPerBlock = 8;   // consecutive tiles per block, at most
 constexpr int kBlocksPerSmTarget = 16; // fewer tiles per block when the group is small
 
-// resident blocks per SM the register budget is sized for (MS: 42 registers)
-template <class M>
-constexpr int min_blocks() { return M::kStates > 4 ? 8 : 12; }
-
-// A block covers tiles [blockIdx.x * tpb, +tpb) of the group's virtual tile
-// space (tpb = 1..8, so that small groups still fill the GPU);
-// consecutive tiles mostly belong to one simulation, so its descriptor, table
-// view and step view are set up once and again only when the walk crosses into
-// the next simulation (the only points where the block syncs).
+// A block walks tiles [blk * tpb, +tpb) of its group's virtual tile space
+// (tpb = 1..8, so that small groups still fill the GPU); consecutive tiles
+// mostly belong to one simulation, so its descriptor, table view and step view
+// are set up once and again only when the walk crosses into the next
+// simulation (the only points where the block syncs).
 template <class M, bool SHARED>
-__global__ void __launch_bounds__(kThreads, min_blocks<M>()) batch_ionic_kernel(const BatchWS* __restrict__ W,
-                                                                                int g, int tpb,
-                                                                                typename M::C c0) {
-    __shared__ MonoDev sd;
-    __shared__ typename M::Tables sT;
-    __shared__ int s_lo;
+__device__ __forceinline__ void ionic_tiles(const BatchWS* __restrict__ W, int g, int tpb, int64_t blk,
+                                            const typename M::C& c0, MonoDev& sd, typename M::Tables& sT,
+                                            int& s_lo) {
     const BatchGroup& G = W->groups[g];
     const int64_t total_tiles = G.tile_prefix[G.count];
-    const int64_t t0 = (int64_t)blockIdx.x * tpb;
+    const int64_t t0 = blk * tpb;
     const int64_t t1 = t0 + tpb < total_tiles ? t0 + tpb : total_tiles;
     int lo = -1;
     int64_t first = 0, next = 0, step = 0;
@@ -81,26 +74,47 @@ __global__ void __launch_bounds__(kThreads, min_blocks<M>()) batch_ionic_kernel(
     }
 }
 
+// Everything one launch needs for every model group of the batch.  A model
+// appears in at most one group, so its shared constant block has a field of its
+// own (read from the constant bank like any kernel argument).
+struct IonicLaunch {
+    const BatchWS* W;
+    int32_t n_groups;
+    int32_t group[kBatchGroups];          // launch order (heavier models first) -> group index
+    int32_t tpb[kBatchGroups];
+    int32_t shared[kBatchGroups];
+    int64_t block_prefix[kBatchGroups + 1];
+    MS::C ms;
+    TTP::C ttp;
+    CRN::C crn;
+};
+
+constexpr size_t kTablesBytes = sizeof(MS::Tables) > sizeof(TTP::Tables)
+                                    ? (sizeof(MS::Tables) > sizeof(CRN::Tables) ? sizeof(MS::Tables) : sizeof(CRN::Tables))
+                                    : (sizeof(TTP::Tables) > sizeof(CRN::Tables) ? sizeof(TTP::Tables) : sizeof(CRN::Tables));
+
 template <class M>
-int launch(const BatchWS* W, int g, int64_t total_tiles, const void* shared_consts, cudaStream_t s) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t per_block = (total_tiles + (int64_t)sms * kBlocksPerSmTarget - 1) / ((int64_t)sms * kBlocksPerSmTarget);
-    const int tpb = (int)(per_block < 1 ? 1 : per_block > kMaxTilesPerBlock ? kMaxTilesPerBlock : per_block);
-    const int64_t blocks = (total_tiles + tpb - 1) / tpb;
-    if (blocks < 1) return TCB_OK;
-    if (blocks > INT32_MAX) return fail(TCB_ERANGE, "batched ionic grid too large");
-    typename M::C c;
-    memset(&c, 0, sizeof c);
-    if (shared_consts) {
-        memcpy(&c, shared_consts, sizeof c);
-        batch_ionic_kernel<M, true><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, tpb, c);
-    } else {
-        batch_ionic_kernel<M, false><<<(unsigned)blocks, kThreads, 0, s>>>(W, g, tpb, c);
+__device__ __forceinline__ void run_group(const IonicLaunch& P, int k, int64_t blk, const typename M::C& c0,
+                                          MonoDev& sd, unsigned char* tabs, int& s_lo) {
+    auto& sT = *reinterpret_cast<typename M::Tables*>(tabs);
+    if (P.shared[k]) ionic_tiles<M, true>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo);
+    else ionic_tiles<M, false>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo);
+}
+
+// One launch for the ionic step of every simulation of the batch: blocks
+// [block_prefix[k], block_prefix[k+1]) run the k-th group's model.
+__global__ void __launch_bounds__(kThreads, 8) batch_ionic_kernel(const IonicLaunch P) {
+    __shared__ MonoDev sd;
+    __shared__ __align__(16) unsigned char tabs[kTablesBytes];
+    __shared__ int s_lo;
+    int k = 0;
+    while (k + 1 < P.n_groups && (int64_t)blockIdx.x >= P.block_prefix[k + 1]) ++k;
+    const int64_t blk = (int64_t)blockIdx.x - P.block_prefix[k];
+    switch (P.W->groups[P.group[k]].model) {
+        case TCB_MODEL_MS: run_group<MS>(P, k, blk, P.ms, sd, tabs, s_lo); break;
+        case TCB_MODEL_TTP: run_group<TTP>(P, k, blk, P.ttp, sd, tabs, s_lo); break;
+        default: run_group<CRN>(P, k, blk, P.crn, sd, tabs, s_lo); break;
     }
-    TCB_CHECK_LAUNCH("batched ionic kernel");
-    return TCB_OK;
 }
 
 }  // namespace
@@ -167,14 +181,46 @@ int model_tables_view(int model, const float* tables, const double* params, void
     return fail(TCB_EINVAL, "unknown ionic model");
 }
 
-int launch_batch_ionic(const BatchWS* ws_dev, const BatchWS& host, int g, int64_t total_tiles,
-                       const void* shared_consts, cudaStream_t s) {
-    switch (host.groups[g].model) {
-        case TCB_MODEL_MS: return launch<MS>(ws_dev, g, total_tiles, shared_consts, s);
-        case TCB_MODEL_TTP: return launch<TTP>(ws_dev, g, total_tiles, shared_consts, s);
-        case TCB_MODEL_CRN: return launch<CRN>(ws_dev, g, total_tiles, shared_consts, s);
+int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* models, const int64_t* tiles,
+                           const int32_t* shared, const char (*consts)[1024], cudaStream_t s) {
+    static_assert(sizeof(IonicLaunch) <= 4000, "kernel argument block");
+    IonicLaunch P;
+    memset(&P, 0, sizeof P);
+    P.W = ws_dev;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // launch order: the heavier models first (TTP, CRN, then MS)
+    int order[kBatchGroups], n = 0;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int g = 0; g < n_groups; ++g)
+            if ((models[g] == TCB_MODEL_MS) == (pass == 1) && tiles[g] > 0) order[n++] = g;
+    P.n_groups = n;
+    int64_t blocks = 0;
+    for (int k = 0; k < n; ++k) {
+        const int g = order[k];
+        const int64_t per = (tiles[g] + (int64_t)sms * kBlocksPerSmTarget - 1) / ((int64_t)sms * kBlocksPerSmTarget);
+        const int tpb = (int)(per < 1 ? 1 : per > kMaxTilesPerBlock ? kMaxTilesPerBlock : per);
+        P.group[k] = g;
+        P.tpb[k] = tpb;
+        P.shared[k] = shared[g];
+        P.block_prefix[k] = blocks;
+        blocks += (tiles[g] + tpb - 1) / tpb;
+        if (shared[g]) {
+            switch (models[g]) {
+                case TCB_MODEL_MS: memcpy(&P.ms, consts[g], sizeof P.ms); break;
+                case TCB_MODEL_TTP: memcpy(&P.ttp, consts[g], sizeof P.ttp); break;
+                case TCB_MODEL_CRN: memcpy(&P.crn, consts[g], sizeof P.crn); break;
+                default: return fail(TCB_EINVAL, "unknown ionic model in batch");
+            }
+        }
     }
-    return fail(TCB_EINVAL, "unknown ionic model in batch");
+    P.block_prefix[n] = blocks;
+    if (blocks < 1) return TCB_OK;
+    if (blocks > INT32_MAX) return fail(TCB_ERANGE, "batched ionic grid too large");
+    batch_ionic_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(P);
+    TCB_CHECK_LAUNCH("batched ionic kernel");
+    return TCB_OK;
 }
 
 }  // namespace tcb
