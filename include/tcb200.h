@@ -259,7 +259,8 @@ typedef struct tcb_batch_plan {
                                  3 = ELL streams staged in shared memory by bulk copies */
     int32_t cg_stage_bytes;   /* staging bytes per warp and stage (variant 3) */
     int32_t cg_stage_ok;      /* 1 if every ELL array allows bulk copies (16-byte aligned) */
-    int32_t pad;
+    int32_t cg_flags;         /* combination (int16 columns 4, A rebuilt 2, linear guess 1) all
+                                 simulations share, or -1: the CG kernel is specialised on it */
     int64_t group_tiles[3];
     int64_t total_slices;
     char group_consts[3][1024];

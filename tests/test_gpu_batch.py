@@ -122,3 +122,29 @@ def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
         got = outputs(s)
         vm = got[2] if "Vm_idx" not in g else got[2][g["Vm_idx"]]
         assert_close(c, (got[0], got[1], vm, got[3]), g["AT"], g["RT"], g["Vm"], int(g["n_total_iter"]))
+
+
+def test_batch_with_mixed_code_paths(lib, cuda, tmp_path):
+    """A batch whose simulations do not share one (int16 columns, A rebuilt,
+    linear guess) combination runs the kernel that picks the path per slice;
+    a uniform batch runs the specialised kernel.  Results as alone."""
+    from torchcor_b200.simulator import MonodomainBatch
+    cases = [C.case(n) for n in ("cube6_ms_f32", "cube8_ttp_f32")]
+    dirs = [case_mesh_dir(c, tmp_path) for c in cases]
+    alone = []
+    for k, (c, d) in enumerate(zip(cases, dirs)):
+        s = build(c, d, cuda)
+        s.solve(c["tol"], c["tol"], c["max_iter"], verbose=False, linear_guess=k == 0)
+        alone.append(outputs(s))
+    batch = MonodomainBatch(cuda)
+    sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"], linear_guess=k == 0)
+            for k, (c, d) in enumerate(zip(cases, dirs))]
+    batch.step(1)
+    assert batch._plan.cg_flags == -1
+    batch.run()
+    for c, s, a in zip(cases, sims, alone):
+        assert_close(c, outputs(s), *a)
+    uniform = MonodomainBatch(cuda)
+    uniform.add(build(cases[0], dirs[0], cuda), 1e-5, 1e-5, 100)
+    uniform.step(1)
+    assert uniform._plan.cg_flags == 7

@@ -56,7 +56,7 @@ class tcb_batch_plan(C.Structure):
         ("workspace", _vp),
         ("n_sims", _i32), ("cg_blocks", _i32), ("cg_smem", _i32), ("n_groups", _i32),
         ("group_model", _i32 * 3), ("group_shared", _i32 * 3), ("cg_variant", _i32), ("cg_stage_bytes", _i32),
-        ("cg_stage_ok", _i32), ("pad", _i32),
+        ("cg_stage_ok", _i32), ("cg_flags", _i32),
         ("group_tiles", _i64 * 3),
         ("total_slices", _i64), ("group_consts", (C.c_char * 1024) * 3),
     ]

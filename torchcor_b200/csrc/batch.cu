@@ -29,8 +29,8 @@ constexpr int kDefaultVariant = 2;    // batched CG variant unless tuned
 size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 // CG grid for S slices: at least kMinSlicesPerBlock slices a block, at most what is resident
-int cg_grid(int64_t S, size_t smem, int variant) {
-    const int cap = batch_cg_max_blocks(smem, variant);
+int cg_grid(int64_t S, size_t smem, int variant, int flags) {
+    const int cap = batch_cg_max_blocks(smem, variant, flags);
     if (cap < 1) return 0;
     const int64_t want = ceil_div(S, cgk::kMinSlicesPerBlock);
     return (int)std::max<int64_t>(1, std::min<int64_t>(want, cap));
@@ -122,13 +122,20 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
         slices[i] = (int32_t)sims[i].n_slices;
         S += sims[i].n_slices;
     }
+    // the combination of per-simulation code paths every simulation shares (or -1)
+    int flags = -1;
+    for (int i = 0; i < n; ++i) {
+        const int f = (views[i].dcol ? 4 : 0) | (views[i].a_split ? 2 : 0) | (views[i].linear_guess ? 1 : 0);
+        flags = i == 0 ? f : (f == flags ? flags : -1);
+        if (flags < 0) break;
+    }
     int variant = kDefaultVariant;
     size_t smem = batch_cg_smem_variant(n, variant);
-    int nb = cg_grid(S, smem, variant);
+    int nb = cg_grid(S, smem, variant, flags);
     if (nb < 1) {
         variant = 1;
         smem = batch_cg_smem_variant(n, variant);
-        nb = cg_grid(S, smem, variant);
+        nb = cg_grid(S, smem, variant, flags);
     }
     if (nb < 1) return fail(TCB_ECUDA, "batched CG kernel cannot be resident");
     // bulk copies need 16-byte aligned sources (slices start at multiples of 32 entries)
@@ -218,7 +225,7 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
     plan->cg_variant = variant;
     plan->cg_stage_bytes = 0;
     plan->cg_stage_ok = stage_ok;
-    plan->pad = 0;
+    plan->cg_flags = flags;
     plan->cg_smem = (int32_t)smem;
     plan->total_slices = S;
     return TCB_OK;
@@ -230,7 +237,7 @@ extern "C" int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant) {
     if (variant == 3 && !plan->cg_stage_ok)
         return fail(TCB_ERANGE, "tcb_batch_set_cg: staged CG needs 16-byte aligned ELL arrays and shared memory");
     const size_t smem = batch_cg_smem_variant(plan->n_sims, variant);
-    const int nb = cg_grid(plan->total_slices, smem, variant);
+    const int nb = cg_grid(plan->total_slices, smem, variant, plan->cg_flags);
     if (nb < 1) return fail(TCB_ERANGE, "tcb_batch_set_cg: that CG variant cannot be resident");
     plan->cg_variant = variant;
     plan->cg_stage_bytes = variant == 3 ? batch_cg_stage_bytes(plan->n_sims) : 0;
@@ -242,7 +249,8 @@ extern "C" int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant) {
 extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream) {
     if (!plan || !plan->workspace || steps < 0) return fail(TCB_EINVAL, "tcb_batch_run: bad arguments");
     if (plan->cg_blocks < 1 || plan->cg_blocks > kBatchMaxBlocks || plan->cg_variant < 1 || plan->cg_variant > 3 ||
-        (plan->cg_variant == 3 && (!plan->cg_stage_ok || plan->cg_stage_bytes < 2048)))
+        (plan->cg_variant == 3 && (!plan->cg_stage_ok || plan->cg_stage_bytes < 2048)) || plan->cg_flags < -1 ||
+        plan->cg_flags > 7)
         return fail(TCB_EINVAL, "tcb_batch_run: plan CG grid out of range");
     cudaStream_t s = as_stream(stream);
     const BatchWS* W = static_cast<const BatchWS*>(plan->workspace);
@@ -250,7 +258,8 @@ extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* st
         int st = launch_batch_ionic_all(W, plan->n_groups, plan->group_model, plan->group_tiles, plan->group_shared,
                                         plan->group_consts, s);
         if (st) return st;
-        st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_variant, plan->cg_stage_bytes, s);
+        st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_variant, plan->cg_stage_bytes,
+                             plan->cg_flags, s);
         if (st) return st;
     }
     return TCB_OK;

@@ -58,10 +58,13 @@ int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* m
                            const int32_t* shared, const char (*consts)[1024], cudaStream_t s);
 // batched CG variants: 1 / 2 = streaming, sized for 1 / 2 blocks per SM;
 // 3 = ELL streams staged in shared memory by bulk copies, 1 block per SM
-int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int stage_bytes, cudaStream_t s);
+// flags: the (int16 columns 4, A rebuilt 2, linear guess 1) combination all the
+// batch's simulations share, or -1 (the streaming variants specialise on it)
+int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int stage_bytes, int flags,
+                    cudaStream_t s);
 size_t batch_cg_smem(int n);
 size_t batch_cg_smem_variant(int n, int variant);
 int batch_cg_stage_bytes(int n);                    // 0 if the staged variant does not fit
-int batch_cg_max_blocks(size_t smem, int variant);  // 0 if that variant cannot be resident
+int batch_cg_max_blocks(size_t smem, int variant, int flags);  // 0 if that variant cannot be resident
 
 }  // namespace tcb

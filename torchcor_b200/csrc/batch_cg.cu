@@ -27,6 +27,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <type_traits>
+
 #include "batch.cuh"
 #include "cg_common.cuh"
 #include "tcb_internal.h"
@@ -49,6 +51,38 @@ template <bool DC>
 __device__ __forceinline__ int col_at(const CgView& d, int64_t e, int row) {
     if constexpr (DC) return row + (int)__ldg(d.dcol + e);
     else return __ldg(d.col + e);
+}
+
+// Call f with std::integral_constant<int, flags> for the simulation's combination
+// of int16 columns (4), A rebuilt from M and K' (2) and linear guess (1): fixed at
+// compile time when the whole batch shares one (FLAGS >= 0), else per slice.
+template <int FLAGS, class F>
+__device__ __forceinline__ void with_flags(const CgView& d, F&& f) {
+    if constexpr (FLAGS >= 0) {
+        f(std::integral_constant<int, FLAGS>{});
+    } else {
+        switch ((d.dcol ? 4 : 0) | (d.a_split ? 2 : 0) | (d.linear_guess ? 1 : 0)) {
+            case 0: f(std::integral_constant<int, 0>{}); break;
+            case 1: f(std::integral_constant<int, 1>{}); break;
+            case 2: f(std::integral_constant<int, 2>{}); break;
+            case 3: f(std::integral_constant<int, 3>{}); break;
+            case 4: f(std::integral_constant<int, 4>{}); break;
+            case 5: f(std::integral_constant<int, 5>{}); break;
+            case 6: f(std::integral_constant<int, 6>{}); break;
+            default: f(std::integral_constant<int, 7>{}); break;
+        }
+    }
+}
+
+// the same for the column format alone (what A p depends on)
+template <int FLAGS, class F>
+__device__ __forceinline__ void with_dcol(const CgView& d, F&& f) {
+    if constexpr (FLAGS >= 0) {
+        f(std::integral_constant<bool, (FLAGS & 4) != 0>{});
+    } else {
+        if (d.dcol) f(std::integral_constant<bool, true>{});
+        else f(std::integral_constant<bool, false>{});
+    }
 }
 
 // Right-hand side, guess, r0 = b - A x0, z0 = D r0 for the 32 rows of slice ls
@@ -690,7 +724,10 @@ constexpr size_t kStageBarBytes = 128 * ((kCgWarps * kStages * 8 + 127) / 128);
 // thread, no spills; 2: 64 registers, twice the warps to hide latency).
 // STAGED: the right-hand side and A p stream their ELL blocks through shared
 // memory by bulk copies (stage_bytes per warp and stage; 1 block per SM).
-template <int PER_SM, bool STAGED>
+// FLAGS: the (int16 columns, A rebuilt, linear guess) combination every
+// simulation of the batch shares (0..7: specialised code, fewer registers), or -1
+// (chosen per slice).
+template <int PER_SM, bool STAGED, int FLAGS>
 __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const BatchWS* __restrict__ W,
                                                                        int stage_bytes) {
     extern __shared__ __align__(128) double smd[];
@@ -731,16 +768,10 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
             W, S, parts0, P, err,
             [&](int i, const CgView& d, int64_t ls, int nk, const unsigned char* buf, Row& rw) {
                 const int step = S.step[i];
-                switch ((d.dcol ? 4 : 0) | (d.a_split ? 2 : 0) | (d.linear_guess ? 1 : 0)) {
-                    case 0: rhs_unit<false, false, false>(d, step, ls, nk, buf, rw, lane); break;
-                    case 1: rhs_unit<false, false, true>(d, step, ls, nk, buf, rw, lane); break;
-                    case 2: rhs_unit<false, true, false>(d, step, ls, nk, buf, rw, lane); break;
-                    case 3: rhs_unit<false, true, true>(d, step, ls, nk, buf, rw, lane); break;
-                    case 4: rhs_unit<true, false, false>(d, step, ls, nk, buf, rw, lane); break;
-                    case 5: rhs_unit<true, false, true>(d, step, ls, nk, buf, rw, lane); break;
-                    case 6: rhs_unit<true, true, false>(d, step, ls, nk, buf, rw, lane); break;
-                    default: rhs_unit<true, true, true>(d, step, ls, nk, buf, rw, lane); break;
-                }
+                with_flags<FLAGS>(d, [&](auto fl) {
+                    constexpr int F = decltype(fl)::value;
+                    rhs_unit<(F & 4) != 0, (F & 2) != 0, (F & 1) != 0>(d, step, ls, nk, buf, rw, lane);
+                });
             },
             [&](int i, const CgView& d, int64_t ls, const Row& rw, double (&acc)[2]) {
                 rhs_end(d, S.step[i], ls, rw, acc, lane);
@@ -748,16 +779,10 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
     } else
     sweep<2>(W, S, parts0, [&](int i, const CgView& d, int64_t ls, double (&acc)[2]) {
         const int step = S.step[i];
-        switch ((d.dcol ? 4 : 0) | (d.a_split ? 2 : 0) | (d.linear_guess ? 1 : 0)) {
-            case 0: rhs_slice<false, false, false>(d, step, ls, lane, acc); break;
-            case 1: rhs_slice<false, false, true>(d, step, ls, lane, acc); break;
-            case 2: rhs_slice<false, true, false>(d, step, ls, lane, acc); break;
-            case 3: rhs_slice<false, true, true>(d, step, ls, lane, acc); break;
-            case 4: rhs_slice<true, false, false>(d, step, ls, lane, acc); break;
-            case 5: rhs_slice<true, false, true>(d, step, ls, lane, acc); break;
-            case 6: rhs_slice<true, true, false>(d, step, ls, lane, acc); break;
-            default: rhs_slice<true, true, true>(d, step, ls, lane, acc); break;
-        }
+        with_flags<FLAGS>(d, [&](auto fl) {
+            constexpr int F = decltype(fl)::value;
+            rhs_slice<(F & 4) != 0, (F & 2) != 0, (F & 1) != 0>(d, step, ls, lane, acc);
+        });
     });
     if (!grid_barrier(W->bar, err)) return;
     totals<2>(W, S, parts0, [&](int i, double* t) {
@@ -778,13 +803,11 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
                 [&](int i, const CgView& d, int64_t ls, int nk, const unsigned char* buf, Row& rw) {
                     const float* pin = (pass & 1) ? d.p2 : d.p;
                     const float beta = (float)S.be[i];
-                    if (d.dcol) {
-                        if (first_pass) ap_unit<true, true>(d, pin, beta, ls, nk, buf, rw, lane);
-                        else ap_unit<true, false>(d, pin, beta, ls, nk, buf, rw, lane);
-                    } else {
-                        if (first_pass) ap_unit<false, true>(d, pin, beta, ls, nk, buf, rw, lane);
-                        else ap_unit<false, false>(d, pin, beta, ls, nk, buf, rw, lane);
-                    }
+                    with_dcol<FLAGS>(d, [&](auto dc) {
+                        constexpr bool DC = decltype(dc)::value;
+                        if (first_pass) ap_unit<DC, true>(d, pin, beta, ls, nk, buf, rw, lane);
+                        else ap_unit<DC, false>(d, pin, beta, ls, nk, buf, rw, lane);
+                    });
                 },
                 [&](int i, const CgView& d, int64_t ls, const Row& rw, double (&acc)[1]) {
                     ap_end(d, (pass & 1) ? d.p2 : d.p, (pass & 1) ? d.p : d.p2, (float)S.be[i], first_pass, ls, rw, acc,
@@ -795,13 +818,11 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
             const float* pin = (pass & 1) ? d.p2 : d.p;
             float* pout = (pass & 1) ? d.p : d.p2;
             const float beta = (float)S.be[i];
-            if (d.dcol) {
-                if (first_pass) ap_slice<true, true>(d, pin, pout, beta, ls, lane, acc);
-                else ap_slice<true, false>(d, pin, pout, beta, ls, lane, acc);
-            } else {
-                if (first_pass) ap_slice<false, true>(d, pin, pout, beta, ls, lane, acc);
-                else ap_slice<false, false>(d, pin, pout, beta, ls, lane, acc);
-            }
+            with_dcol<FLAGS>(d, [&](auto dc) {
+                constexpr bool DC = decltype(dc)::value;
+                if (first_pass) ap_slice<DC, true>(d, pin, pout, beta, ls, lane, acc);
+                else ap_slice<DC, false>(d, pin, pout, beta, ls, lane, acc);
+            });
         });
         if (!grid_barrier(W->bar, err)) return;
         totals<1>(W, S, parts1, [&](int i, double* t) { S.al[i] = S.rz[i] / t[0]; });
@@ -851,21 +872,36 @@ size_t batch_cg_smem(int n) { return carve_bytes(n); }
 
 namespace {
 
+using KernelFn = void (*)(const BatchWS*, int);
+
+// the kernel of a variant (1, 2: streaming; 3: staged) and flag combination
+// (-1 or 0..7); the streaming variants have a specialisation per combination
 template <int PER_SM, bool STAGED>
-int max_blocks(size_t smem) {
-    int dev = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaFuncSetAttribute(batch_cg_kernel<PER_SM, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_cg_kernel<PER_SM, STAGED>, kCgThreads, smem) !=
-            cudaSuccess) {
-        cudaGetLastError();
-        return 0;
+KernelFn pick(int flags) {
+    if constexpr (STAGED) {
+        return batch_cg_kernel<PER_SM, STAGED, -1>;
+    } else {
+        switch (flags) {
+            case 0: return batch_cg_kernel<PER_SM, false, 0>;
+            case 1: return batch_cg_kernel<PER_SM, false, 1>;
+            case 2: return batch_cg_kernel<PER_SM, false, 2>;
+            case 3: return batch_cg_kernel<PER_SM, false, 3>;
+            case 4: return batch_cg_kernel<PER_SM, false, 4>;
+            case 5: return batch_cg_kernel<PER_SM, false, 5>;
+            case 6: return batch_cg_kernel<PER_SM, false, 6>;
+            case 7: return batch_cg_kernel<PER_SM, false, 7>;
+        }
+        return batch_cg_kernel<PER_SM, false, -1>;
     }
-    if (occ > PER_SM) occ = PER_SM;
-    const int cap = sms * occ;
-    return cap > kBatchMaxBlocks ? kBatchMaxBlocks : cap;
+}
+
+KernelFn kernel_of(int variant, int flags) {
+    switch (variant) {
+        case 1: return pick<1, false>(flags);
+        case 2: return pick<2, false>(flags);
+        case 3: return pick<1, true>(flags);
+    }
+    return nullptr;
 }
 
 }  // namespace
@@ -887,16 +923,29 @@ size_t batch_cg_smem_variant(int n, int variant) {
     return carve_bytes(n) + kStageBarBytes + (size_t)kCgWarps * kStages * batch_cg_stage_bytes(n);
 }
 
-int batch_cg_max_blocks(size_t smem, int variant) {
-    switch (variant) {
-        case 1: return max_blocks<1, false>(smem);
-        case 2: return max_blocks<2, false>(smem);
-        case 3: return max_blocks<1, true>(smem);
+// Blocks of `variant` that fit with `smem` bytes of shared memory (0 if none);
+// also sets the shared-memory attribute of the kernel the plan will launch.
+int batch_cg_max_blocks(size_t smem, int variant, int flags) {
+    const KernelFn k = kernel_of(variant, flags);
+    if (!k) return 0;
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kCgThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
     }
-    return 0;
+    const int per_sm = variant == 2 ? 2 : 1;
+    if (occ > per_sm) occ = per_sm;
+    const int cap = sms * occ;
+    return cap > kBatchMaxBlocks ? kBatchMaxBlocks : cap;
 }
 
-int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int stage_bytes, cudaStream_t s) {
+int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int stage_bytes, int flags,
+                    cudaStream_t s) {
+    const KernelFn k = kernel_of(variant, flags);
+    if (!k) return fail(TCB_EINVAL, "unknown batched CG variant");
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nb);
     cfg.blockDim = dim3(kCgThreads);
@@ -907,12 +956,7 @@ int launch_batch_cg(const BatchWS* ws_dev, int nb, size_t smem, int variant, int
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (variant == 1)
-        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<1, false>, ws_dev, 0));
-    else if (variant == 2)
-        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<2, false>, ws_dev, 0));
-    else
-        TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, batch_cg_kernel<1, true>, ws_dev, stage_bytes));
+    TCB_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k, ws_dev, variant == 3 ? stage_bytes : 0));
     return TCB_OK;
 }
 
