@@ -221,8 +221,8 @@ def tcb_arm(a, wl, world, rank, local):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # the timed steps replay CUDA graphs of G steps (Monodomain.capture_steps), the
     # remainder runs as plain launches
-    G = a.graph_steps if a.graph_steps > 0 else 0
-    replay = sim.capture_steps(G) if G and a.steps >= G else None
+    G = a.graph_steps if 0 < a.graph_steps <= a.steps else 0
+    replay = sim.capture_steps(G) if G else None
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
@@ -345,22 +345,25 @@ def batch_arm(a, world, rank, local):
         tuned = tune_batch(batch, steps=10)[1]
         torch.cuda.synchronize(dev)
     cg_cfg = batch.cg_config
-    G = a.graph_steps
-    replay = batch.capture(G) if G > 0 else None
+    # the timed steps replay CUDA graphs of G steps, the remainder runs as plain launches
+    G = a.graph_steps if 0 < a.graph_steps <= a.steps else 0
+    replay = batch.capture(G) if G else None
     if replay:
         replay()
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    K = a.steps if not replay else (a.steps // G) * G
+    K = a.steps
     if world > 1:
         torch.distributed.barrier()
     with ClockSampler(local) as clk:
         e0.record(stream)
+        done = 0
         if replay:
             for _ in range(K // G):
                 replay()
-        else:
-            batch.step(K)
+            done = (K // G) * G
+        if K > done:
+            batch.step(K - done)
         e1.record(stream)
         torch.cuda.synchronize(dev)
     ms = replicas.reduce_max(e0.elapsed_time(e1))     # slowest rank (each rank runs the batch)

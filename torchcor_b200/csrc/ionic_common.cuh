@@ -79,6 +79,24 @@ TCB_HD float lut_col(const Lut& L, const LutPos& p, int c) {
     return p.w1 * ldro(r0 + c) + p.w * ldro(r0 + S + c);
 }
 
+// columns c and c + 1 (c even) of the interpolated row, each table row read as one
+// 8-byte vector; the table starts 16-byte aligned and its stride is even, so the
+// pair is 8-byte aligned.  Same arithmetic as two lut_col calls.
+template <int NCOL>
+TCB_HD float2 lut_pair(const Lut& L, const LutPos& p, int c) {
+    constexpr int S = lut_stride(NCOL);
+    static_assert(S % 2 == 0, "paired columns need an even stride");
+    const float* r0 = L.tab + (int64_t)p.lo * S + c;
+#ifdef __CUDA_ARCH__
+    const float2 a = __ldg(reinterpret_cast<const float2*>(r0));
+    const float2 b = __ldg(reinterpret_cast<const float2*>(r0 + S));
+#else
+    const float2 a = make_float2(r0[0], r0[1]);
+    const float2 b = make_float2(r0[S], r0[S + 1]);
+#endif
+    return make_float2(p.w1 * a.x + p.w * b.x, p.w1 * a.y + p.w * b.y);
+}
+
 // every column of the interpolated row, the two table rows read as 16-byte vectors
 template <int NCOL>
 TCB_HD void lut_row(const Lut& L, const LutPos& p, float* out) {

@@ -31,6 +31,15 @@ enum TTPV {
     TV_M_A, TV_M_B, TV_R_A, TV_R_B, TV_S_A, TV_S_B, TV_Xr1_A, TV_Xr1_B, TV_Xr2_A, TV_Xr2_B, TV_Xs_A, TV_Xs_B,
     TV_a2, TV_rec_iNaK, TV_rec_ipK, TV_NCOL
 };
+// columns read as pairs (lut_pair): (X_A, X_B) of every V gate, (INaCa_A, INaCa_B) and
+// (a2, rec_iNaK); each pair starts at an even column with its partner next to it
+static_assert(TV_D_A % 2 == 0 && TV_F2_A % 2 == 0 && TV_F_A % 2 == 0 && TV_H_A % 2 == 0 && TV_INaCa_A % 2 == 0 &&
+              TV_J_A % 2 == 0 && TV_M_A % 2 == 0 && TV_R_A % 2 == 0 && TV_S_A % 2 == 0 && TV_Xr1_A % 2 == 0 &&
+              TV_Xr2_A % 2 == 0 && TV_Xs_A % 2 == 0 && TV_a2 % 2 == 0 && TV_rec_iNaK == TV_a2 + 1,
+              "paired V-table columns");
+
+// Rush-Larsen update x' = A + B * x from the interpolated (A, B) pair
+TCB_HD float rl_gate(float2 ab, float x) { return ab.x + ab.y * x; }
 enum TTPS { S_CaSR, S_CaSS, S_Cai, S_D, S_F, S_F2, S_FCaSS, S_H, S_J, S_Ki, S_M, S_Nai, S_R, S_R_, S_S, S_Xr1,
             S_Xr2, S_Xs, TTP_NS };
 
@@ -275,22 +284,23 @@ struct TTP {
         float IpCa = (c.GpCa * Cai) / (Cai + c.KpCa);
         float v15 = V - 15.0f;
         float a1 = c.ga1 * ((V == 15.0f) ? c.halfFRT : v15 / expm1f((2.0f * v15) * c.F_RT));
-        float ICaL_A = a1 * lut_col<TV_NCOL>(T.V, pv, TV_a2);
+        const float2 a2_iNaK = lut_pair<TV_NCOL>(T.V, pv, TV_a2);  // TV_a2, TV_rec_iNaK
+        float ICaL_A = a1 * a2_iNaK.x;
         float ICaL_B = a1 * c.Cao;
         float VmEk = V - Ek;
         float IKr = ((c.GKr_sqrtKo * s[S_Xr1]) * s[S_Xr2]) * VmEk;
         float IKs = ((c.GKs * s[S_Xs]) * s[S_Xs]) * (V - Eks);
         float m = s[S_M];
         float INa = (((((c.GNa * m) * m) * m) * s[S_H]) * s[S_J]) * (V - Ena);
-        float INaK = (c.pmf_INaK * (Nai / (Nai + c.KmNa))) * lut_col<TV_NCOL>(T.V, pv, TV_rec_iNaK);
+        float INaK = (c.pmf_INaK * (Nai / (Nai + c.KmNa))) * a2_iNaK.y;
         float IbCa = c.GbCa * (V - Eca);
         float IbNa = c.GbNa * (V - Ena);
         float IpK = (c.GpK * lut_col<TV_NCOL>(T.V, pv, TV_rec_ipK)) * VmEk;
         float Ito = ((c.Gto * s[S_R]) * s[S_S]) * VmEk;
         LutPos pe = lut_pos(VmEk, T.VEk);
         float ICaL = (((s[S_D] * s[S_F]) * s[S_F2]) * s[S_FCaSS]) * ((ICaL_A * CaSS) - ICaL_B);
-        float INaCa = (((lut_col<TV_NCOL>(T.V, pv, TV_INaCa_A) * Nai) * Nai) * Nai) -
-                      (lut_col<TV_NCOL>(T.V, pv, TV_INaCa_B) * Cai);
+        const float2 naca = lut_pair<TV_NCOL>(T.V, pv, TV_INaCa_A);
+        float INaCa = (((naca.x * Nai) * Nai) * Nai) - (naca.y * Cai);
         float IK1 = (c.GK1 * lut_col<1>(T.VEk, pe, 0)) * VmEk;
         float Iion = ((((((((((IKr + IKs) + IK1) + Ito) + INa) + IbNa) + ICaL) + IbCa) + INaK) + INaCa) + IpCa) + IpK;
 
@@ -323,18 +333,18 @@ struct TTP {
         s[S_Nai] = Nai + diff_Nai * c.dt;
         s[S_R_] = R_ + diff_R_ * c.dt;
         // Rush-Larsen (:439-450)
-        s[S_D] = lut_col<TV_NCOL>(T.V, pv, TV_D_A) + lut_col<TV_NCOL>(T.V, pv, TV_D_B) * s[S_D];
-        s[S_F] = lut_col<TV_NCOL>(T.V, pv, TV_F_A) + lut_col<TV_NCOL>(T.V, pv, TV_F_B) * s[S_F];
-        s[S_F2] = lut_col<TV_NCOL>(T.V, pv, TV_F2_A) + lut_col<TV_NCOL>(T.V, pv, TV_F2_B) * s[S_F2];
+        s[S_D] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_D_A), s[S_D]);
+        s[S_F] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_F_A), s[S_F]);
+        s[S_F2] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_F2_A), s[S_F2]);
         s[S_FCaSS] = lut_col<3>(T.CaSS, pc, 1) + lut_col<3>(T.CaSS, pc, 2) * s[S_FCaSS];
-        s[S_H] = lut_col<TV_NCOL>(T.V, pv, TV_H_A) + lut_col<TV_NCOL>(T.V, pv, TV_H_B) * s[S_H];
-        s[S_J] = lut_col<TV_NCOL>(T.V, pv, TV_J_A) + lut_col<TV_NCOL>(T.V, pv, TV_J_B) * s[S_J];
-        s[S_M] = lut_col<TV_NCOL>(T.V, pv, TV_M_A) + lut_col<TV_NCOL>(T.V, pv, TV_M_B) * m;
-        s[S_R] = lut_col<TV_NCOL>(T.V, pv, TV_R_A) + lut_col<TV_NCOL>(T.V, pv, TV_R_B) * s[S_R];
-        s[S_S] = lut_col<TV_NCOL>(T.V, pv, TV_S_A) + lut_col<TV_NCOL>(T.V, pv, TV_S_B) * s[S_S];
-        s[S_Xr1] = lut_col<TV_NCOL>(T.V, pv, TV_Xr1_A) + lut_col<TV_NCOL>(T.V, pv, TV_Xr1_B) * s[S_Xr1];
-        s[S_Xr2] = lut_col<TV_NCOL>(T.V, pv, TV_Xr2_A) + lut_col<TV_NCOL>(T.V, pv, TV_Xr2_B) * s[S_Xr2];
-        s[S_Xs] = lut_col<TV_NCOL>(T.V, pv, TV_Xs_A) + lut_col<TV_NCOL>(T.V, pv, TV_Xs_B) * s[S_Xs];
+        s[S_H] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_H_A), s[S_H]);
+        s[S_J] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_J_A), s[S_J]);
+        s[S_M] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_M_A), m);
+        s[S_R] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_R_A), s[S_R]);
+        s[S_S] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_S_A), s[S_S]);
+        s[S_Xr1] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_Xr1_A), s[S_Xr1]);
+        s[S_Xr2] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_Xr2_A), s[S_Xr2]);
+        s[S_Xs] = rl_gate(lut_pair<TV_NCOL>(T.V, pv, TV_Xs_A), s[S_Xs]);
         return -Iion;
     }
 };
