@@ -74,3 +74,17 @@ def test_device_pattern_equals_host_pattern(lib, cuda, mesh):
     assert g.nnz == h.nnz
     for name in ("rowptr", "col", "slot_ptr", "slot_src", "diag"):
         assert np.array_equal(g.host(name), h.host(name)), name
+
+
+def test_pattern_row_beyond_device_cap_uses_host_build(lib, cuda):
+    """A fan of 400 triangles around node 0 puts 1,200 element contributions in row 0,
+    more than one device sort takes: the build falls back to the host and still
+    equals it."""
+    from torchcor_b200.core.assemble import build_pattern
+    m = 400
+    el = np.array([(0, 1 + i, 1 + (i + 1) % m) for i in range(m)], dtype=np.int32)
+    h = build_pattern(el, m + 1)
+    g = build_pattern(torch.from_numpy(el).to(cuda), m + 1)
+    assert g.nnz == h.nnz == (1 + m) + 4 * m      # hub row, rim rows (self, hub, two neighbours)
+    for name in ("rowptr", "col", "slot_ptr", "slot_src", "diag"):
+        assert np.array_equal(g.host(name), h.host(name)), name

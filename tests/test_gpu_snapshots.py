@@ -14,10 +14,10 @@ from tests.test_gpu_reorder import _build
 pytestmark = pytest.mark.gpu
 
 
-def _run(case, d, cuda, tmp, ring, interval, reorder=False):
+def _run(case, d, cuda, tmp, ring, interval, reorder=False, graph_steps=100):
     sim = _build(case, d, cuda, reorder)
     sim.solve(case["tol"], case["tol"], case["max_iter"], verbose=False, snapshot_interval=interval,
-              result_path=tmp, snapshot_ring=ring)
+              result_path=tmp, snapshot_ring=ring, graph_steps=graph_steps)
     return sim
 
 
@@ -38,3 +38,20 @@ def test_streamed_snapshots_equal_device_snapshots(lib, cuda, tmp_path, name, in
     assert torch.equal(got.activation_time.cpu(), ref.activation_time.cpu())
     assert torch.equal(got.repolarization_time.cpu(), ref.repolarization_time.cpu())
     assert torch.equal(torch.load(tmp_path / "b" / "Vm.pt"), torch.load(tmp_path / "a" / "Vm.pt"))
+
+
+@pytest.mark.parametrize("name,interval,ring,graph_steps", [
+    ("cube6_ms_f32", 1.0, None, 7),       # whole loop in one chunk: 1 plain step, 7-step replays, a plain tail
+    ("cube6_ms_f32", 1.0, 2, 7),          # streamed snapshots: replays inside every 100-step frame
+    ("ico3_crn_f32", 2.0, None, 100),
+])
+def test_graph_replay_equals_plain_launches(lib, cuda, tmp_path, name, interval, ring, graph_steps):
+    case = C.case(name)
+    d = case_mesh_dir(case, tmp_path)
+    ref = _run(case, d, cuda, tmp_path / "a", ring, interval, graph_steps=0)
+    got = _run(case, d, cuda, tmp_path / "b", ring, interval, graph_steps=graph_steps)
+    assert got._sim.get("graph") is not None and ref._sim.get("graph") is None
+    assert torch.equal(got.solutions.cpu(), ref.solutions.cpu())
+    assert torch.equal(got.activation_time.cpu(), ref.activation_time.cpu())
+    assert torch.equal(got.repolarization_time.cpu(), ref.repolarization_time.cpu())
+    assert torch.equal(got._sim["step_iters"].cpu(), ref._sim["step_iters"].cpu())

@@ -53,9 +53,19 @@ class Pattern:
 def build_pattern(elems, n_nodes: int) -> Pattern:
     """CSR pattern (equal to the reference's coalesce -> to_sparse_csr) and the
     contribution map in the reference's COO order: host C++ for a numpy array,
-    the device build (same arrays, bit for bit) for a CUDA tensor."""
+    the device build (same arrays, bit for bit) for a CUDA tensor, the host build
+    for a CUDA tensor with a row beyond the device build's 1024 contributions."""
     if isinstance(elems, torch.Tensor):
-        return build_pattern_device(elems, n_nodes)
+        if not elems.is_cuda:
+            elems = elems.numpy()
+        else:
+            try:
+                return build_pattern_device(elems, n_nodes)
+            except _lib.TcbError as e:
+                if e.status != _lib.TCB_ERANGE:
+                    raise
+                # a row with more element contributions than the device sort takes
+                elems = elems.cpu().numpy()
     lib = _lib.load()
     el = np.ascontiguousarray(elems, dtype=np.int32)
     E, k = el.shape

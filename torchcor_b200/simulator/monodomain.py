@@ -117,9 +117,11 @@ class Monodomain:
             self.node_order = perm
             self._perm_t = torch.from_numpy(perm).to(self.device)
             self._inv_t = torch.from_numpy(inv).to(self.device)
-        self._elems_np = np.ascontiguousarray(elems, dtype=np.int32)
+        elems = np.ascontiguousarray(elems, dtype=np.int32)
         self.nodes = torch.from_numpy(np.ascontiguousarray(nodes)).to(dtype=torch.float32, device=self.device)
-        self.elems = torch.from_numpy(self._elems_np).to(device=self.device)
+        self.elems = torch.from_numpy(elems).to(device=self.device)
+        # the assembly pattern is built where the elements are (the device build on a GPU)
+        self._elems_np = self.elems if self.elems.is_cuda else elems
         self.regions = torch.from_numpy(np.ascontiguousarray(regions)).to(dtype=torch.int, device=self.device)
         self.fibres = torch.from_numpy(np.ascontiguousarray(fibres)).to(dtype=torch.float32, device=self.device)
         self.stimuli = Stimuli(self.n_nodes, self.device, self.dtype)
@@ -226,6 +228,22 @@ class Monodomain:
         sim["next_step"] = b
         return b - a
 
+    def _advance(self, n, graph_steps):
+        """Run ``n`` steps: whole ``graph_steps``-step stretches replay one CUDA graph
+        (recorded on first use, after a plain launch has configured the kernels), the
+        rest run as plain launches."""
+        sim = self._sim
+        G = int(graph_steps or 0)
+        if G > 1 and n >= G:
+            rep = sim.get("graph")
+            if rep is None or rep.n_steps != G:
+                n -= self.run_steps(1)
+                rep = sim["graph"] = self.capture_steps(G)
+            while n >= G:
+                rep()
+                n -= G
+        self.run_steps(n)
+
     def capture_steps(self, n_steps):
         """Record ``n_steps`` steps of the prepared simulation in a CUDA graph;
         returns a callable replaying them (with the step bookkeeping)."""
@@ -242,6 +260,7 @@ class Monodomain:
             graph.replay()
             sim["next_step"] += n_steps
         replay.graph = graph
+        replay.n_steps = n_steps
         return replay
 
     def _stim_bits(self):
@@ -445,11 +464,14 @@ class Monodomain:
                            snapshot_interval < self.T)
 
     def solve(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1,
-              verbose=True, result_path=None, snapshot_ring=None):
+              verbose=True, result_path=None, snapshot_ring=None, graph_steps=100):
         """monodomain.py:141-226.  ``snapshot_ring=R`` keeps only R snapshot frames on
         the device and streams every frame, as soon as it is written, into a pinned host
         tensor on a separate stream (``solutions`` is then that host tensor); the
-        default keeps every frame on the device, as the reference does."""
+        default keeps every frame on the device, as the reference does.
+        ``graph_steps=G`` runs every whole G-step stretch of the loop as the replay of
+        one CUDA graph of the same kernels (recorded once per solve); the results are
+        bit-identical to plain launches (``graph_steps=0``)."""
         self.result_path = Path(result_path) if result_path is not None else None
         if self.result_path is not None:
             self.result_path.mkdir(parents=True, exist_ok=True)
@@ -467,9 +489,10 @@ class Monodomain:
         else:
             chunk = max(1, sim["per_frame"]) * (1 if verbose and snapshot_interval != self.T else 1000)
         while sim["next_step"] <= self.nt:
+            n = min(chunk, self.nt + 1 - sim["next_step"])
             if ring:
-                self._before_steps(sim["next_step"], min(chunk, self.nt + 1 - sim["next_step"]))
-            self.run_steps(chunk)
+                self._before_steps(sim["next_step"], n)
+            self._advance(n, graph_steps)
             if ring:
                 self._drain_snapshots()
             if verbose and snapshot_interval != self.T:
