@@ -30,6 +30,7 @@
 #include <cstdlib>
 
 #include "cg_common.cuh"
+#include "l2_hint.cuh"
 #include "mono.cuh"
 #include "tcb_internal.h"
 
@@ -39,14 +40,15 @@ namespace {
 using namespace cgk;
 
 template <typename IDX>
-__device__ __forceinline__ int col_at(const IDX* __restrict__ col, int64_t e, int64_t row);
+__device__ __forceinline__ int col_at(const IDX* __restrict__ col, int64_t e, int64_t row, uint64_t pol);
 template <>
-__device__ __forceinline__ int col_at<int32_t>(const int32_t* __restrict__ col, int64_t e, int64_t) {
-    return __ldg(col + e);
+__device__ __forceinline__ int col_at<int32_t>(const int32_t* __restrict__ col, int64_t e, int64_t, uint64_t pol) {
+    return ld_hint(col + e, pol);
 }
 template <>
-__device__ __forceinline__ int col_at<int16_t>(const int16_t* __restrict__ col, int64_t e, int64_t row) {
-    return (int)row + (int)__ldg(col + e);
+__device__ __forceinline__ int col_at<int16_t>(const int16_t* __restrict__ col, int64_t e, int64_t row,
+                                               uint64_t pol) {
+    return (int)row + ld_hint(col + e, pol);
 }
 
 // p_new = z + beta * p_old in float32 (one fused multiply-add, beta rounded to
@@ -82,6 +84,7 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
     double* parts0 = d.scratch;
     double* parts1 = d.scratch + 2 * kMaxBlocks;
     const bool lg = d.linear_guess != 0;
+    const uint64_t keep = l2_keep(), once = l2_once();
 
     // ---- right-hand side, guess, r0, z0 (solver.py:46-55; monodomain.py:130-131)
     double acc2[2] = {0.0, 0.0};
@@ -102,10 +105,10 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
             for (int j = 0; j < 4; ++j) {
                 const bool ok = k0 + j < w;
                 const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
-                c[j] = ok ? col_at<IDX>(col, e, row) : (int)row;
-                mv[j] = ok ? __ldg(d.mv + e) : 0.0f;
-                kv[j] = ok ? __ldg(d.kv + e) : 0.0f;
-                av[j] = ok ? (ASPLIT ? __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]) : __ldg(d.av + e)) : 0.0f;
+                c[j] = ok ? col_at<IDX>(col, e, row, keep) : (int)row;
+                mv[j] = ok ? ld_hint(d.mv + e, once) : 0.0f;
+                kv[j] = ok ? ld_hint(d.kv + e, once) : 0.0f;
+                av[j] = ok ? (ASPLIT ? __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]) : ld_hint(d.av + e, keep)) : 0.0f;
             }
             float bc[4], uc[4], xc[4];
 #pragma unroll
@@ -166,8 +169,8 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
                 for (int j = 0; j < 8; ++j) {
                     const bool ok = k0 + j < w;
                     const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
-                    c[j] = ok ? col_at<IDX>(col, e, row) : (int)row;
-                    av[j] = ok ? __ldg(d.av + e) : 0.0f;
+                    c[j] = ok ? col_at<IDX>(col, e, row, keep) : (int)row;
+                    av[j] = ok ? ld_hint(d.av + e, keep) : 0.0f;
                 }
                 float zc[8], pc[8];
 #pragma unroll

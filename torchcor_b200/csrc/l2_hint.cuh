@@ -1,0 +1,46 @@
+// L2 eviction priorities for the per-step streams (createpolicy + L2::cache_hint).
+//
+// A monodomain step moves more bytes than the 126 MB L2 holds: the ionic state
+// (read and written once a step), M and K (read once a step by the right-hand
+// side) and the column offsets and A values (read by every CG pass of every step;
+// 91 MB for a million-node cube).  The CG kernel loads the last group as
+// last-to-go and M and K as first-to-go, which keeps the reused data in L2 across
+// passes and steps.  Hints only: no result depends on them.
+#pragma once
+
+#include <stdint.h>
+
+namespace tcb {
+
+// policy for data read again by later passes and steps
+__device__ __forceinline__ uint64_t l2_keep() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// policy for data touched once a step
+__device__ __forceinline__ uint64_t l2_once() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// read-only (non-coherent path) loads of data no thread writes during the kernel
+__device__ __forceinline__ float ld_hint(const float* a, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_hint(const int32_t* a, uint64_t pol) {
+    int v;
+    asm volatile("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_hint(const int16_t* a, uint64_t pol) {
+    short v;
+    asm volatile("ld.global.nc.L2::cache_hint.s16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
+    return (int)v;
+}
+
+}  // namespace tcb
