@@ -18,6 +18,9 @@
 //  * the right-hand side phase does not stream A when the assembly verified that
 //    every A value equals fp32(fp32(M*Cm) + K') bit for bit (true for theta =
 //    0.5, the reference's value): the coefficient is rebuilt from M and K';
+//  * the column offsets and A are loaded as L2 evict-last, M and K as evict-first
+//    (l2_hint.cuh), so the offsets the right-hand side read are still in L2 when
+//    the A p phase reads them again;
 //  * z and p of neighbouring rows are read through L1 after the grid barrier
 //    (whose gpu-scope fences order them after the writers' stores).
 // All float32 values that neighbours see (z, p) are rounded once and every row

@@ -2,10 +2,12 @@
 //
 // A monodomain step moves more bytes than the 126 MB L2 holds: the ionic state
 // (read and written once a step), M and K (read once a step by the right-hand
-// side) and the column offsets and A values (read by every CG pass of every step;
-// 91 MB for a million-node cube).  The CG kernel loads the last group as
-// last-to-go and M and K as first-to-go, which keeps the reused data in L2 across
-// passes and steps.  Hints only: no result depends on them.
+// side) and the column offsets and A values (read by every CG pass; 91 MB for a
+// million-node cube).  The CG kernel loads the column offsets and A as
+// last-to-go and M and K as first-to-go.  Measured on that cube (DRAM bytes of a
+// launch with warm caches), the column offsets the right-hand side read are still
+// in L2 for the A p phase; A itself and anything across steps are not.  Hints
+// only: no result depends on them.
 #pragma once
 
 #include <stdint.h>
