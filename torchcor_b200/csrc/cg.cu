@@ -28,7 +28,7 @@ namespace {
 
 using namespace cgk;
 
-__global__ void __launch_bounds__(kCgThreads) cg_kernel(MonoDev d) {
+__global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
     __shared__ double sh_part[kCgWarps * 2];
     __shared__ double sh_tot[2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -89,15 +89,32 @@ __device__ __forceinline__ void block_partial(double (&v)[NV], double* parts, do
     }
 }
 
-// Sum of all blocks' partials; every block computes the same value.
+// Sum of all blocks' partials; every block computes the same value.  Each lane
+// adds the partials of blocks lane, lane + 32, ... in that order; the loads of
+// eight strides are issued before their adds, so a lane waits for one L2 round
+// trip per eight strides instead of one per stride (same sums, bit for bit).
 template <int NV>
 __device__ __forceinline__ void grid_total(const double* parts, double (&out)[NV], double* sh) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) {
+        constexpr int kBatch = 8;
         double acc[NV];
 #pragma unroll
         for (int i = 0; i < NV; ++i) acc[i] = 0.0;
-        for (unsigned b = lane; b < gridDim.x; b += 32)
+        const unsigned nb = gridDim.x;
+        unsigned b = lane;
+        for (; b + 32 * (kBatch - 1) < nb; b += 32 * kBatch) {
+            double t[kBatch][NV];
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k)
+#pragma unroll
+                for (int i = 0; i < NV; ++i) t[k][i] = __ldcg(parts + (b + 32 * k) * NV + i);
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k)
+#pragma unroll
+                for (int i = 0; i < NV; ++i) acc[i] += t[k][i];
+        }
+        for (; b < nb; b += 32)
 #pragma unroll
             for (int i = 0; i < NV; ++i) acc[i] += __ldcg(parts + b * NV + i);
 #pragma unroll
