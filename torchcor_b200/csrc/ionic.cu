@@ -135,7 +135,7 @@ __global__ void differentiate_kernel(typename M::C c, typename M::Tables T, floa
 }
 
 template <class M>
-__global__ void __launch_bounds__(kThreads) mono_ionic_kernel(MonoDev d, typename M::C c, typename M::Tables T) {
+__global__ void __launch_bounds__(kThreads, M::kMinBlocksPerSm) mono_ionic_kernel(MonoDev d, typename M::C c, typename M::Tables T) {
     const StepView sv = step_view(d, d.counter[0]);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += (int64_t)gridDim.x * blockDim.x)
         ionic_node<M>(d, c, T, sv, i);

@@ -37,6 +37,10 @@ enum CRNS { R_Ca_rel, R_Ca_up, R_Cai, R_Ki, R_d, R_f, R_f_Ca, R_h, R_j, R_m, R_o
 
 struct CRN {
     static constexpr int kStates = CRN_NS;
+    // 256-thread blocks per SM the single-simulation ionic kernel is compiled for: 3
+    // (80 registers, 60 bytes of spills) against 1 unbounded (218 registers): 0.059 ->
+    // 0.033 ms a launch on a 531,441-node cube on B200; 2 and 4 measured slower
+    static constexpr int kMinBlocksPerSm = 3;
     static constexpr LutSpec kCai{3e-4, 30.0, 3e-4, CC_NCOL};
     static constexpr LutSpec kV{-200.0, 200.0, 0.1, CV_NCOL};
     static constexpr LutSpec kFn{-2e-11, 10.0e-11, 2e-15, 3};

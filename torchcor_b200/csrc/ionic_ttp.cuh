@@ -45,6 +45,10 @@ enum TTPS { S_CaSR, S_CaSS, S_Cai, S_D, S_F, S_F2, S_FCaSS, S_H, S_J, S_Ki, S_M,
 
 struct TTP {
     static constexpr int kStates = TTP_NS;
+    // 256-thread blocks per SM the single-simulation ionic kernel is compiled for: 6
+    // (40 registers, 76 bytes of spills) beats 4 (64 registers, none) by 1 % on B200;
+    // 5 measured slower
+    static constexpr int kMinBlocksPerSm = 6;
     static constexpr LutSpec kV{-800.0, 800.0, 0.05, TV_NCOL};
     static constexpr LutSpec kCaSS{0.00001, 10.0, 0.00001, 3};
     static constexpr LutSpec kVEk{-800.0, 800.0, 0.05, 1};
