@@ -145,9 +145,9 @@ def oracle_sim(wl):
     return sim
 
 
-def time_oracle(wl, budget_s, min_steps=2, max_steps=None):
-    """Oracle on the workload: assembly (timed separately), then steps until
-    ``budget_s`` seconds of stepping (at least ``min_steps``)."""
+def time_oracle(wl, budget_s, min_steps=2, max_steps=None, warmup=0):
+    """Oracle on the workload: assembly (timed separately), ``warmup`` untimed
+    steps, then steps until ``budget_s`` seconds of stepping (at least ``min_steps``)."""
     cores = os.cpu_count() or 1
     torch.set_num_threads(cores)
     sim = oracle_sim(wl)
@@ -157,15 +157,19 @@ def time_oracle(wl, budget_s, min_steps=2, max_steps=None):
     u = sim.ionic.initialize(sim.n_nodes)
     sim.cg.initialize(u, linear_guess=True)
     t = 0.0
+    warmup = min(warmup, wl.nt - 1)
+    for _ in range(warmup):
+        t += wl.dt
+        u, _ = sim.step(u, t, 1e-5, 1e-5, 100)
     n = 0
     el = 0.0
-    while (el < budget_s or n < min_steps) and (max_steps is None or n < max_steps) and n < wl.nt:
+    while (el < budget_s or n < min_steps) and (max_steps is None or n < max_steps) and n + warmup < wl.nt:
         t += wl.dt
         t1 = time.perf_counter()
         u, _ = sim.step(u, t, 1e-5, 1e-5, 100)
         el += time.perf_counter() - t1
         n += 1
-    return dict(value=wl.n_nodes * n / el, steps=n, seconds=el, assemble_s=t_asm, cores=cores)
+    return dict(value=wl.n_nodes * n / el, steps=n, seconds=el, assemble_s=t_asm, cores=cores, warmup=warmup)
 
 
 def reference_arm(a, wl, world, rank):
@@ -174,12 +178,12 @@ def reference_arm(a, wl, world, rank):
     # warm-up steps are run untimed inside the same oracle session; the timed
     # sample is bounded to keep the whole run within a few minutes
     budget = float(os.environ.get("TCB_REFERENCE_BUDGET_S", "60"))
-    r = time_oracle(wl, budget_s=budget, min_steps=min(a.steps, 3), max_steps=a.steps)
+    r = time_oracle(wl, budget_s=budget, min_steps=min(a.steps, 3), max_steps=a.steps, warmup=a.warmup)
     v = r["value"]
     sample = (f"oracle (CPU restatement of the reference path, torch CPU, {r['cores']} threads) on the full "
-              f"workload: assembly {r['assemble_s']:.1f} s untimed, then {r['steps']} timed steps "
-              f"({r['seconds']:.1f} s)")
-    line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world, "steps": r["steps"], "warmup": 0,
+              f"workload: assembly {r['assemble_s']:.1f} s and {r['warmup']} warm-up steps untimed, then "
+              f"{r['steps']} timed steps ({r['seconds']:.1f} s)")
+    line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world, "steps": r["steps"], "warmup": r["warmup"],
             "ms_per_step": 1000 * r["seconds"] / r["steps"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": wl.name, "nodes": wl.n_nodes, "elements": int(len(wl.elems)), "dt_ms": wl.dt,
@@ -288,10 +292,11 @@ def tcb_arm(a, wl, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        r = time_oracle(wl, budget_s=float(os.environ.get("TCB_CPU_BASELINE_S", "15")), min_steps=3)
+        r = time_oracle(wl, budget_s=float(os.environ.get("TCB_CPU_BASELINE_S", "15")), min_steps=3, warmup=3)
         cpu = {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": "port",
                "sample": f"oracle on the full workload, {r['steps']} steps after an untimed "
-                         f"{r['assemble_s']:.1f} s assembly ({r['seconds']:.1f} s of stepping)"}
+                         f"{r['assemble_s']:.1f} s assembly and {r['warmup']} untimed warm-up steps "
+                         f"({r['seconds']:.1f} s of stepping)"}
     if rank != 0:
         return
     line = {
