@@ -29,6 +29,7 @@
 
 #include <type_traits>
 
+#include "l2_hint.cuh"
 #include "batch.cuh"
 #include "cg_common.cuh"
 #include "tcb_internal.h"
@@ -46,11 +47,14 @@ __device__ __forceinline__ float p_update(float z, float p_old, float beta, bool
     return first ? z : __fmaf_rn(beta, p_old, z);
 }
 
-// column of ELL entry e of `row`: int16 offset from the row or int32 index
+// column of ELL entry e of `row`: int16 offset from the row or int32 index.  The
+// matrix streams (columns, M, K, A) of a batch are far larger than L2 and read
+// once a pass: they are loaded as first to leave L2, ahead of the row vectors the
+// neighbour gathers reuse.
 template <bool DC>
 __device__ __forceinline__ int col_at(const CgView& d, int64_t e, int row) {
-    if constexpr (DC) return row + (int)__ldg(d.dcol + e);
-    else return __ldg(d.col + e);
+    if constexpr (DC) return row + ld_hint_sched(d.dcol + e, l2_once_sched());
+    else return ld_hint_sched(d.col + e, l2_once_sched());
 }
 
 // Call f with std::integral_constant<int, flags> for the simulation's combination
@@ -116,9 +120,9 @@ __device__ __forceinline__ void rhs_slice(const CgView& d, int step, int64_t ls,
         for (int j = 0; j < 4; ++j) {
             const bool ok = k0 + j < w;
             const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
-            mv[j] = ok ? __ldg(d.mv + e) : 0.0f;
-            kv[j] = ok ? __ldg(d.kv + e) : 0.0f;
-            if constexpr (!AS) av[j] = ok ? __ldg(d.av + e) : 0.0f;
+            mv[j] = ok ? ld_hint_sched(d.mv + e, l2_once_sched()) : 0.0f;
+            kv[j] = ok ? ld_hint_sched(d.kv + e, l2_once_sched()) : 0.0f;
+            if constexpr (!AS) av[j] = ok ? ld_hint_sched(d.av + e, l2_once_sched()) : 0.0f;
             bc[j] = __ldg(bp + c[j]);
             uc[j] = __ldg(u + c[j]);
             if constexpr (LG) xc[j] = __ldg(xp + c[j]);
@@ -179,7 +183,7 @@ __device__ __forceinline__ void ap_slice(const CgView& d, const float* pin, floa
             const bool ok = k0 + j < w;
             const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
             c[j] = ok ? col_at<DC>(d, e, r) : r;
-            av[j] = ok ? __ldg(d.av + e) : 0.0f;
+            av[j] = ok ? ld_hint_sched(d.av + e, l2_once_sched()) : 0.0f;
         }
         float zc[8], pc[8];
 #pragma unroll

@@ -28,7 +28,15 @@ __device__ __forceinline__ uint64_t l2_once() {
     return p;
 }
 
-// read-only (non-coherent path) loads of data no thread writes during the kernel
+// Read-only (non-coherent path) loads of data no thread writes during the kernel,
+// in two forms, because the two CG kernels need opposite ones (measured on B200):
+//  * ld_hint: volatile asm, issued in program order where written.  The resident
+//    CG kernel relies on that: with the plain form the compiler rescheduled its
+//    loads and a launch on a million-node cube went from 0.099 to 0.128 ms;
+//  * ld_hint_sched (with l2_once_sched): plain asm without a memory clobber, which
+//    the compiler schedules like __ldg.  The batched CG kernel needs that for its
+//    column prefetch: with the volatile form a 64-cube batch step took 1.21 ms
+//    instead of 0.70.
 __device__ __forceinline__ float ld_hint(const float* a, uint64_t pol) {
     float v;
     asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
@@ -42,6 +50,29 @@ __device__ __forceinline__ int ld_hint(const int32_t* a, uint64_t pol) {
 __device__ __forceinline__ int ld_hint(const int16_t* a, uint64_t pol) {
     short v;
     asm volatile("ld.global.nc.L2::cache_hint.s16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
+    return (int)v;
+}
+
+
+// the schedulable form (see above)
+__device__ __forceinline__ uint64_t l2_once_sched() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ float ld_hint_sched(const float* a, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_hint_sched(const int32_t* a, uint64_t pol) {
+    int v;
+    asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_hint_sched(const int16_t* a, uint64_t pol) {
+    short v;
+    asm("ld.global.nc.L2::cache_hint.s16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
     return (int)v;
 }
 
