@@ -221,3 +221,54 @@ def test_rcm_order_is_a_bandwidth_reducing_permutation():
     inv[p] = np.arange(len(p))
     bw = lambda e: max(np.abs(e[:, i] - e[:, j]).max() for i in range(3) for j in range(3))  # noqa: E731
     assert bw(inv[tris]) * 10 < bw(tris)
+
+
+def test_pattern_from_cpu_tensor_equals_numpy(lib):
+    """build_pattern takes a CPU tensor like a numpy array (host build)."""
+    from torchcor_b200 import meshgen
+    from torchcor_b200.core.assemble import build_pattern
+    nodes, elems = meshgen.cube(5, 1.0)
+    h = build_pattern(elems, len(nodes))
+    t = build_pattern(torch.from_numpy(np.ascontiguousarray(elems, dtype=np.int32)), len(nodes))
+    assert t.nnz == h.nnz
+    for name in ("rowptr", "col", "slot_ptr", "slot_src", "diag"):
+        assert np.array_equal(t.host(name), h.host(name)), name
+
+
+def test_solve_loop_graph_replay_accounting():
+    """The solve loop's step runner: one plain step before the graph is recorded,
+    then whole G-step replays and the rest as plain launches; the graph is recorded
+    once per prepared run; G = 0 or a stretch shorter than G runs plain launches."""
+    from torchcor_b200.simulator import Monodomain
+
+    class Fake:
+        def __init__(self):
+            self._sim, self.log = {}, []
+
+        def run_steps(self, n):
+            if n:
+                self.log.append(("plain", n))
+            return n
+
+        def capture_steps(self, g):
+            self.log.append(("capture", g))
+
+            def replay():
+                self.log.append(("replay", g))
+            replay.n_steps = g
+            return replay
+
+    f = Fake()
+    Monodomain._advance(f, 1000, 7)
+    assert f.log[:2] == [("plain", 1), ("capture", 7)]
+    assert f.log.count(("replay", 7)) == 142 and f.log[-1] == ("plain", 5)
+    assert sum(k for op, k in f.log if op != "capture") == 1000
+    f.log.clear()
+    Monodomain._advance(f, 100, 7)
+    assert ("capture", 7) not in f.log and f.log.count(("replay", 7)) == 14 and f.log[-1] == ("plain", 2)
+    f.log.clear()
+    Monodomain._advance(f, 5, 7)
+    assert f.log == [("plain", 5)]
+    g = Fake()
+    Monodomain._advance(g, 50, 0)
+    assert g.log == [("plain", 50)]
