@@ -18,9 +18,10 @@
 //  * the right-hand side phase does not stream A when the assembly verified that
 //    every A value equals fp32(fp32(M*Cm) + K') bit for bit (true for theta =
 //    0.5, the reference's value): the coefficient is rebuilt from M and K';
-//  * the column offsets and A are loaded as L2 evict-last, M and K as evict-first
-//    (l2_hint.cuh), so the offsets the right-hand side read are still in L2 when
-//    the A p phase reads them again;
+//  * the column offsets are loaded as L2 evict-last, M, K and A as evict-first
+//    (l2_hint.cuh), so the offsets stay in L2 from the right-hand side through
+//    every A p pass; marking A evict-last as well (61 MB more on a million-node
+//    cube) pushed the offsets and row vectors out and cost 10 % a launch;
 //  * z and p of neighbouring rows are read through L1 after the grid barrier
 //    (whose gpu-scope fences order them after the writers' stores).
 // All float32 values that neighbours see (z, p) are rounded once and every row
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
                 c[j] = ok ? col_at<IDX>(col, e, row, keep) : (int)row;
                 mv[j] = ok ? ld_hint(d.mv + e, once) : 0.0f;
                 kv[j] = ok ? ld_hint(d.kv + e, once) : 0.0f;
-                av[j] = ok ? (ASPLIT ? __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]) : ld_hint(d.av + e, keep)) : 0.0f;
+                av[j] = ok ? (ASPLIT ? __fadd_rn(__fmul_rn(mv[j], d.cm), kv[j]) : ld_hint(d.av + e, once)) : 0.0f;
             }
             float bc[4], uc[4], xc[4];
 #pragma unroll
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
                     const bool ok = k0 + j < w;
                     const int64_t e = base + (int64_t)(k0 + j) * TCB_SLICE;
                     c[j] = ok ? col_at<IDX>(col, e, row, keep) : (int)row;
-                    av[j] = ok ? ld_hint(d.av + e, keep) : 0.0f;
+                    av[j] = ok ? ld_hint(d.av + e, once) : 0.0f;
                 }
                 float zc[8], pc[8];
 #pragma unroll

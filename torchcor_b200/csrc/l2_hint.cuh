@@ -3,11 +3,10 @@
 // A monodomain step moves more bytes than the 126 MB L2 holds: the ionic state
 // (read and written once a step), M and K (read once a step by the right-hand
 // side) and the column offsets and A values (read by every CG pass; 91 MB for a
-// million-node cube).  The CG kernel loads the column offsets and A as
-// last-to-go and M and K as first-to-go.  Measured on that cube (DRAM bytes of a
-// launch with warm caches), the column offsets the right-hand side read are still
-// in L2 for the A p phase; A itself and anything across steps are not.  Hints
-// only: no result depends on them.
+// million-node cube).  The resident CG kernel loads the column offsets (30 MB) as
+// last-to-go and M, K and A as first-to-go, so the offsets the right-hand side
+// read stay in L2 through the A p passes; with A last-to-go too the set no longer
+// fitted and a launch took 10 % longer.  Hints only: no result depends on them.
 #pragma once
 
 #include <stdint.h>
