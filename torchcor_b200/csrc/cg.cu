@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "cg_common.cuh"
+#include "l2_hint.cuh"
 #include "mono.cuh"
 #include "tcb_internal.h"
 
@@ -48,6 +49,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
     double* parts0 = d.scratch;
     double* parts1 = d.scratch + 2 * kMaxBlocks;
     const bool lg = d.linear_guess != 0;
+    const uint64_t once = l2_once();   // M, K and A: first to leave L2
 
     // ---- right-hand side, initial guess, r0, z0 = p0 (solver.py:46-55; monodomain.py:130-131)
     double acc2[2] = {0.0, 0.0};  // ||D b||^2, r.z
@@ -64,9 +66,9 @@ __global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
             const int c = __ldg(d.col + e);
             const float uc = u[c];
             const float xg = lg ? 2.0f * uc - xp[c] : uc;
-            mb = __fmaf_rn(__ldg(d.mv + e), bp[c], mb);
-            ku = __fmaf_rn(__ldg(d.kv + e), uc, ku);
-            ax += (double)__ldg(d.av + e) * (double)xg;
+            mb = __fmaf_rn(ld_hint(d.mv + e, once), bp[c], mb);
+            ku = __fmaf_rn(ld_hint(d.kv + e, once), uc, ku);
+            ax += (double)ld_hint(d.av + e, once) * (double)xg;
         }
         const float rhs = mb - ku;
         const float ui = u[row];
@@ -99,7 +101,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
             double a = 0.0;
             for (int k = 0; k < w; ++k) {
                 const int64_t e = base + (int64_t)k * TCB_SLICE;
-                a += (double)__ldg(d.av + e) * (double)__ldcg(p + __ldg(d.col + e));
+                a += (double)ld_hint(d.av + e, once) * (double)__ldcg(p + __ldg(d.col + e));
             }
             const float a32 = (float)a;
             ap[row] = a32;
