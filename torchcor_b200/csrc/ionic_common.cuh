@@ -97,28 +97,6 @@ TCB_HD float2 lut_pair(const Lut& L, const LutPos& p, int c) {
     return make_float2(p.w1 * a.x + p.w * b.x, p.w1 * a.y + p.w * b.y);
 }
 
-// every column of the interpolated row, the two table rows read as 16-byte vectors
-template <int NCOL>
-TCB_HD void lut_row(const Lut& L, const LutPos& p, float* out) {
-    constexpr int S = lut_stride(NCOL);
-    static_assert(S % 4 == 0, "vector rows need a stride that is a multiple of 4");
-    const float* r0 = L.tab + (int64_t)p.lo * S;
-#ifdef __CUDA_ARCH__
-    float a[S], b[S];
-#pragma unroll
-    for (int q = 0; q < S / 4; ++q) {
-        const float4 x = __ldg(reinterpret_cast<const float4*>(r0) + q);
-        const float4 y = __ldg(reinterpret_cast<const float4*>(r0 + S) + q);
-        a[4 * q] = x.x; a[4 * q + 1] = x.y; a[4 * q + 2] = x.z; a[4 * q + 3] = x.w;
-        b[4 * q] = y.x; b[4 * q + 1] = y.y; b[4 * q + 2] = y.z; b[4 * q + 3] = y.w;
-    }
-#pragma unroll
-    for (int c = 0; c < NCOL; ++c) out[c] = p.w1 * a[c] + p.w * b[c];
-#else
-    for (int c = 0; c < NCOL; ++c) out[c] = p.w1 * r0[c] + p.w * r0[S + c];
-#endif
-}
-
 // host-side helpers describing a table the way the reference does
 struct LutSpec {
     double mn, mx, res;
