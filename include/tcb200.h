@@ -139,11 +139,12 @@ int tcb_model_layout(int32_t model, const double* params, int64_t* n_states, int
  * starting at float offset `offset`.  TCB_ERANGE past the last table. */
 int tcb_model_table_info(int32_t model, int32_t index, int64_t* rows, int32_t* ncol, int32_t* stride,
                          int64_t* offset);
-/* construct_tables (TTP :197-318, CRN :212-328); no-op for MS */
+/* construct_tables (TTP :197-318, CRN :212-328); no-op for MS.  `tables` must be
+ * 16-byte aligned (TCB_EINVAL otherwise), as in every call that reads it. */
 int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream);
 /* initialize(n_nodes): fill state rows and V with the initial values */
 int tcb_model_init(int32_t model, const double* params, float* state, int64_t n_pad, float* v, void* stream);
-/* differentiate(V): dv = -Iion and the state update, for n nodes */
+/* differentiate(V): dv = -Iion and the state update, for n nodes (`tables` 16-byte aligned) */
 int tcb_model_differentiate(int32_t model, const double* params, const float* tables, float* state,
                             int64_t n_pad, int64_t n, const float* v, float* dv, void* stream);
 
@@ -166,7 +167,7 @@ typedef struct tcb_mono {
     const float* d_inv;      /* 1/diag(A) */
     /* ionic */
     float* state;
-    const float* tables;
+    const float* tables;     /* 16-byte aligned (TCB_EINVAL otherwise); unused for MS */
     /* vectors (n_pad each; x is 3*n_pad) */
     float* x;
     float* bprime;

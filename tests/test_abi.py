@@ -272,3 +272,16 @@ def test_solve_loop_graph_replay_accounting():
     g = Fake()
     Monodomain._advance(g, 50, 0)
     assert g.log == [("plain", 50)]
+
+
+def test_misaligned_tables_rejected_before_any_launch(lib):
+    """The ionic kernels read table column pairs as 8-byte vectors: a table pointer
+    that is not 16-byte aligned is refused on the host (no device access happens,
+    so fake addresses are enough here)."""
+    from torchcor_b200 import _lib
+    model = _lib.MODEL_TTP
+    params = np.zeros(len(_lib.model_params(model)), dtype=np.float64)
+    fake = 1 << 20
+    st = lib.tcb_model_differentiate(model, _lib.ptr(params), fake + 4, fake, 1, 1, fake, fake, None)
+    assert st == _lib.TCB_EINVAL
+    assert lib.tcb_model_tables(model, _lib.ptr(params), fake + 8, None) == _lib.TCB_EINVAL

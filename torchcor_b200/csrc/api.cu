@@ -85,6 +85,9 @@ int validate(const tcb_mono* m) {
         !m->step_stim || !m->step_iters || !m->counter || !m->scratch || !m->barrier || !m->params)
         return fail(TCB_EINVAL, "tcb_mono: null pointer");
     if (m->model != TCB_MODEL_MS && !m->tables) return fail(TCB_EINVAL, "tcb_mono: null tables");
+    // the ionic kernels read table column pairs as 8-byte vectors
+    if (m->model != TCB_MODEL_MS && ((uintptr_t)m->tables & 15u))
+        return fail(TCB_EINVAL, "tcb_mono: tables not 16-byte aligned");
     if (m->max_iter < 0 || m->per_frame < 0 || m->snap_ring < 0)
         return fail(TCB_EINVAL, "tcb_mono: negative max_iter/per_frame/snap_ring");
     return TCB_OK;

@@ -269,6 +269,7 @@ extern "C" int tcb_model_tables(int32_t model, const double* params, float* tabl
     cudaStream_t s = as_stream(stream);
     if (model == TCB_MODEL_MS) return TCB_OK;
     if (!tables) return fail(TCB_EINVAL, "tcb_model_tables: null tables");
+    if ((uintptr_t)tables & 15u) return fail(TCB_EINVAL, "tcb_model_tables: tables not 16-byte aligned");
     if (model == TCB_MODEL_TTP) {
         TTP::C c = TTP::derive(params);
         TTP::Tables T = TTP::tables(tables, params);
@@ -313,6 +314,8 @@ extern "C" int tcb_model_differentiate(int32_t model, const double* params, cons
                                        int64_t n_pad, int64_t n, const float* v, float* dv, void* stream) {
     if (!params || !state || !v || !dv || n <= 0 || n_pad < n) return fail(TCB_EINVAL, "tcb_model_differentiate: bad arguments");
     if (model != TCB_MODEL_MS && !tables) return fail(TCB_EINVAL, "tcb_model_differentiate: null tables");
+    if (model != TCB_MODEL_MS && ((uintptr_t)tables & 15u))
+        return fail(TCB_EINVAL, "tcb_model_differentiate: tables not 16-byte aligned");
     cudaStream_t s = as_stream(stream);
     switch (model) {
         case TCB_MODEL_MS: return run_differentiate<MS>(params, tables, state, n_pad, n, v, dv, s);
