@@ -73,9 +73,40 @@ CASES = [
          stim=50.0, stim_start=0.0, stim_dur=2.0),
 ]
 
+# Full-size runs of the benchmark workloads, stored compactly (``compact``):
+# activation/repolarisation times as step indices for every node, Vm at a few
+# frames on a seeded node sample plus per-frame statistics of every node, the
+# CSR pattern as a SHA-256 digest, per-step CG iteration counts.  They take
+# tens of minutes of reference CPU time each and are generated on request
+# (``make_golden.py --only <name>``).
+_CFG2 = dict(kind="tissue", model="ttp", cell_type="ENDO",
+             mesh=dict(type="cube", n=100, h=0.25, fibres="rotz", regions="splitx"), conductivity=_TTP_COND,
+             stimuli=[dict(file="c0.vtx", nodes=dict(type="corner", k=5, seed=1234, which=0), start=0.0,
+                           duration=1.0, intensity=100),
+                      dict(file="c1.vtx", nodes=dict(type="corner", k=5, seed=1234, which=1), start=5.0,
+                           duration=1.0, intensity=100)],
+             dt=0.01, T=40.0, tol=1e-5, max_iter=100, big=True,
+             compact=dict(seed=5, vm_sample=32768, vm_frames=[1, 2, 5, 6, 10, 20, 30, 40]))
+_CFG3 = dict(kind="tissue", model="crn", mesh=dict(type="ico", level=7, radius=25.0, fibres="tangent", seed=7),
+             conductivity=[dict(region_ids=[1], il=0.4, it=0.1)],
+             stimuli=[dict(file="cap.vtx", nodes=dict(type="zcap", frac=0.98), start=0.0, duration=2.0,
+                           intensity=50)],
+             dt=0.02, T=400.0, tol=1e-5, max_iter=100, big=True,
+             compact=dict(seed=5, vm_sample=32768, vm_frames=[1, 2, 4, 10, 50, 100, 200, 300, 350, 400]))
+
+BIG_CASES = [
+    # TTP ENDO on the 100^3-cell cube (1,030,301 nodes): the single-simulation benchmark workload
+    # over its first 40 ms (4,000 steps: both stimuli, the fronts crossing the cube)
+    dict(_CFG2, name="cfg2_ttp_f32", dtype="f32"),
+    dict(_CFG2, name="cfg2_ttp_f64", dtype="f64"),
+    # CRN on the level-7 icosphere (163,842 nodes), run through repolarisation (T = 400 ms)
+    dict(_CFG3, name="cfg3_crn_f32", dtype="f32"),
+    dict(_CFG3, name="cfg3_crn_f64", dtype="f64"),
+]
+
 
 def case(name):
-    for c in CASES:
+    for c in CASES + BIG_CASES:
         if c["name"] == name:
             return c
     raise KeyError(name)

@@ -1,9 +1,14 @@
 """Generate the golden fixtures in this directory by running the TorchCor
 reference itself (pure Python/PyTorch, CPU).
 
-Run from the repository root, where the reference checkout is mounted:
+Run from the repository root, pointing at a TorchCor checkout (``--ref`` or
+the ``TORCHCOR_REF`` environment variable):
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--only name ...]
+    python tests/golden/make_golden.py --ref <torchcor checkout> [--only name ...]
+
+The full-size cases (``cases.BIG_CASES``: the 1,030,301-node TTP cube and the
+level-7 CRN icosphere, each in float32 and float64) take tens of minutes of
+CPU time each and run only when named with ``--only``.
 
 The reference is imported with small stubs for its post-processing imports
 (pyvista, matplotlib, the ECG module) and with NVML/``torch.cuda`` calls in
@@ -16,7 +21,9 @@ inputs of every case so the tests can rebuild them without the reference.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
+import os
 import sys
 import tempfile
 import time
@@ -86,12 +93,18 @@ def run_tissue(md, ionic, case, workdir):
     iters = []
     orig_step = sim.step
     traj = []
+    step_wall = []
 
     def step(u, t, a_tol, r_tol, max_iter, verbose=False):
+        t0 = time.perf_counter()
         out = orig_step(u, t, a_tol, r_tol, max_iter, verbose)
+        step_wall.append(time.perf_counter() - t0)
         iters.append(out[1])
         if len(traj) < case.get("keep_steps", 0):
             traj.append(out[0].clone())
+        if case.get("big") and len(iters) % 500 == 0:
+            print(f"  {case['name']}: step {len(iters)}, t={t:.2f}, {np.mean(step_wall[-500:]) * 1e3:.1f} ms/step, "
+                  f"{sum(iters)} CG iterations", flush=True)
         return out
 
     sim.step = step
@@ -107,6 +120,8 @@ def run_tissue(md, ionic, case, workdir):
     RT = torch.load(out_dir / "RTs.pt").numpy()
     Vm = torch.load(out_dir / "Vm.pt").numpy()
     A = sim.A
+    if case.get("compact"):
+        return compact_fixture(case, sim, AT, RT, Vm, total, iters, wall, step_wall)
     fx = dict(AT=AT, RT=RT, n_total_iter=np.int64(total), iters=np.asarray(iters, dtype=np.int16),
               crow=A.crow_indices().numpy().astype(np.int32), col=A.col_indices().numpy().astype(np.int32),
               wall=np.float64(wall))
@@ -134,6 +149,45 @@ def run_tissue(md, ionic, case, workdir):
         for k, v in st.items():
             fx["state_" + k] = v
     return fx
+
+
+def pattern_digest(crow, col):
+    """SHA-256 of the CSR pattern as little-endian int32 rowptr then column bytes."""
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(crow, dtype="<i4").tobytes())
+    h.update(np.ascontiguousarray(col, dtype="<i4").tobytes())
+    return h.hexdigest()
+
+
+def time_steps(times, dt):
+    """Activation/repolarisation times -> step index n (t_n = n * dt accumulated), -1 where unset."""
+    times = np.asarray(times, dtype=np.float64)
+    steps = np.where(times < 0, -1, np.rint(times / dt)).astype(np.int64)
+    assert steps.max() < 32768
+    return steps.astype(np.int16)
+
+
+def compact_fixture(case, sim, AT, RT, Vm, total, iters, wall, step_wall):
+    """Fixture of a full-size case: every node's AT/RT as step indices, Vm on a
+    seeded node sample at the listed frames, per-frame statistics over all nodes,
+    the pattern digest, matrix sums, per-step iteration counts, reference timing."""
+    cp = case["compact"]
+    n = AT.shape[0]
+    idx = np.sort(np.random.default_rng(cp["seed"]).choice(n, size=min(cp["vm_sample"], n), replace=False))
+    frames = np.asarray(cp["vm_frames"], dtype=np.int32)
+    Vm64 = Vm.astype(np.float64)
+    A = sim.A
+    return dict(AT_step=time_steps(AT, case["dt"]), RT_step=time_steps(RT, case["dt"]),
+                n_total_iter=np.int64(total), iters=np.asarray(iters, dtype=np.int16),
+                pattern_sha256=np.array(pattern_digest(A.crow_indices().numpy(), A.col_indices().numpy())),
+                nnz=np.int64(A.col_indices().numel()),
+                M_sum=np.float64(sim.M.values().double().sum()),
+                K_abs_sum=np.float64(sim.K.values().double().abs().sum()),
+                A_sum=np.float64(sim.A.values().double().sum()),
+                Vm_nodes=idx.astype(np.int32), Vm_idx=frames, Vm=Vm[frames][:, idx],
+                Vm_absmax=np.abs(Vm64).max(axis=1), Vm_mean=Vm64.mean(axis=1), Vm_min=Vm64.min(axis=1),
+                wall=np.float64(wall), step_seconds=np.float64(np.sum(step_wall)),
+                threads=np.int64(torch.get_num_threads()))
 
 
 def states_of(im, model):
@@ -190,17 +244,20 @@ def run_cell(ionic, case):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("TORCHCOR_REF"),
+                    help="TorchCor checkout to import (default: $TORCHCOR_REF)")
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--threads", type=int, default=8)
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the TorchCor checkout with --ref or TORCHCOR_REF")
     torch.set_num_threads(a.threads)
     md, ionic = import_reference(a.ref)
     with open(HERE / "cases.json", "w") as f:
-        json.dump(C.CASES, f, indent=1)
+        json.dump(C.CASES + C.BIG_CASES, f, indent=1)
     with tempfile.TemporaryDirectory() as work:
-        for case in C.CASES:
-            if a.only and case["name"] not in a.only:
+        for case in C.CASES + C.BIG_CASES:
+            if (a.only and case["name"] not in a.only) or (case.get("big") and not a.only):
                 continue
             t0 = time.time()
             kind = case["kind"]

@@ -285,3 +285,22 @@ def test_misaligned_tables_rejected_before_any_launch(lib):
     st = lib.tcb_model_differentiate(model, _lib.ptr(params), fake + 4, fake, 1, 1, fake, fake, None)
     assert st == _lib.TCB_EINVAL
     assert lib.tcb_model_tables(model, _lib.ptr(params), fake + 8, None) == _lib.TCB_EINVAL
+
+
+def test_mitchell_schaeffer_constructor_forms(lib):
+    """MitchellSchaeffer(device, dtype) (the reference's form, dt from the simulator)
+    and MitchellSchaeffer(dt, device=..., dtype=...) give ModifiedMS2v's parameters."""
+    from torchcor_b200 import ionic
+    ref_form = ionic.MitchellSchaeffer(torch.device("cpu"), torch.float32)
+    assert ref_form.dt is None and ref_form.device == torch.device("cpu") and ref_form.dtype == torch.float32
+    str_form = ionic.MitchellSchaeffer("cpu")
+    assert str_form.dt is None and str_form.device == torch.device("cpu")
+    with_dt = ionic.MitchellSchaeffer(0.02, device="cpu", dtype=torch.float32)
+    assert with_dt.dt == 0.02
+    base = ionic.ModifiedMS2v(0.02, device="cpu")
+    ref_form.dt = 0.02
+    assert np.array_equal(ref_form.param_array(), base.param_array())
+    assert np.array_equal(with_dt.param_array(), base.param_array())
+    assert ref_form.name == "MitchellSchaeffer" and isinstance(ref_form, ionic.ModifiedMS2v)
+    with pytest.raises(NotImplementedError):
+        ionic.MitchellSchaeffer(torch.device("cpu"), torch.float64)
