@@ -139,6 +139,13 @@ int tcb_model_layout(int32_t model, const double* params, int64_t* n_states, int
  * starting at float offset `offset`.  TCB_ERANGE past the last table. */
 int tcb_model_table_info(int32_t model, int32_t index, int64_t* rows, int32_t* ncol, int32_t* stride,
                          int64_t* offset);
+/* Instances of the fused per-step ionic kernel for `model` (no counterpart in the reference: launch
+ * shapes an autotuner chooses between, all computing the same per-node arithmetic): *count
+ * instances; instance `variant` (1..count, 0 = the default) handles *nodes_per_thread consecutive
+ * nodes per thread (structure-of-arrays state moved as 4-, 8- or 16-byte vectors) with the register
+ * budget of *blocks_per_sm 256-thread blocks per SM.  TCB_ERANGE past the last instance. */
+int tcb_ionic_variant(int32_t model, int32_t variant, int32_t* count, int32_t* nodes_per_thread,
+                      int32_t* blocks_per_sm);
 /* construct_tables (TTP :197-318, CRN :212-328); no-op for MS.  `tables` must be
  * 16-byte aligned (TCB_EINVAL otherwise), as in every call that reads it. */
 int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream);
@@ -192,6 +199,12 @@ typedef struct tcb_mono {
     float cm, dt;
     int32_t snap_ring;       /* 0: snapshots holds every frame; > 0: rows in the snapshot ring (the
                                 caller copies each frame out before it is overwritten) */
+    /* launch shapes (no counterpart in the reference; chosen by measurement) */
+    int32_t ionic_variant;   /* ionic kernel instance, 1..count of tcb_ionic_variant(); 0 = the default.
+                                Instances with more than one node per thread need x, state, bprime, at, rt
+                                and stim_bits aligned to the vector (else the first one-node instance runs) */
+    int32_t cg_per_sm;       /* blocks per SM of the CG kernel that keeps rows in shared memory: 0 = the
+                                most whose rows fit (2, else 1); 1 or 2 pins it */
     /* device bookkeeping (caller-allocated, zero-initialised) */
     int32_t* step_iters;     /* [nt+1] CG iterations of each step */
     int32_t* counter;        /* [4]: next step, error code, 2 spare */

@@ -44,7 +44,7 @@ class tcb_mono(C.Structure):
         ("stim_bits", _vp), ("step_t", _vp), ("step_stim", _vp), ("stim_amp", C.c_float * TCB_MAX_STIMULI),
         ("a_tol", _f64), ("r_tol", _f64),
         ("max_iter", _i32), ("linear_guess", _i32), ("at_rt", _i32), ("per_frame", _i32), ("a_split", _i32),
-        ("cm", C.c_float), ("dt", C.c_float), ("snap_ring", _i32),
+        ("cm", C.c_float), ("dt", C.c_float), ("snap_ring", _i32), ("ionic_variant", _i32), ("cg_per_sm", _i32),
         ("step_iters", _vp), ("counter", _vp), ("scratch", _vp), ("barrier", _vp),
         ("params", _vp),
     ]
@@ -85,6 +85,7 @@ SIGNATURES = [
     ("tcb_model_states", C.c_char_p, [_i32]),
     ("tcb_model_layout", C.c_int, [_i32, _vp, _pi64, _pi64]),
     ("tcb_model_table_info", C.c_int, [_i32, _i32, _pi64, C.POINTER(_i32), C.POINTER(_i32), _pi64]),
+    ("tcb_ionic_variant", C.c_int, [_i32, _i32, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
     ("tcb_model_tables", C.c_int, [_i32, _vp, _vp, _vp]),
     ("tcb_model_init", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp]),
     ("tcb_model_differentiate", C.c_int, [_i32, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp]),
@@ -177,3 +178,16 @@ def table_layout(model):
 
 def model_states(model):
     return load().tcb_model_states(model).decode().split(",")
+
+
+def ionic_variants(model):
+    """[(nodes_per_thread, blocks_per_sm)] of the model's ionic kernel instances
+    (instance k + 1 in ``tcb_mono.ionic_variant``); entry 0 is the default."""
+    lib = load()
+    cnt, v, b = C.c_int32(), C.c_int32(), C.c_int32()
+    check(lib.tcb_ionic_variant(model, 0, C.byref(cnt), C.byref(v), C.byref(b)))
+    out = []
+    for k in range(1, cnt.value + 1):
+        check(lib.tcb_ionic_variant(model, k, C.byref(cnt), C.byref(v), C.byref(b)))
+        out.append((v.value, b.value))
+    return out

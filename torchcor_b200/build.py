@@ -24,8 +24,9 @@ BUILD = PKG / "_build"
 LIB = PKG / "libtcb200.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# translation units that must keep float32 expressions as separate roundings
-NO_FMA = {"ionic.cu", "batch_ionic.cu"}
+# translation units that must keep float32 expressions as separate roundings (the
+# lookup-table builders: their grids pass through removable singularities)
+NO_FMA = {"tables.cu"}
 
 
 def _nvcc():

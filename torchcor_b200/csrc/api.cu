@@ -1,5 +1,6 @@
 // Status handling and the time-loop entry points of the C ABI.
 #include <cuda_runtime.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <string>
@@ -52,7 +53,7 @@ MonoDev make_dev(const tcb_mono* m) {
     d.rt = m->rt;
     d.snap = m->snapshots;
     d.snap_ring = m->snap_ring;
-    d.pad = 0;
+    d.cg_per_sm = m->cg_per_sm;
     d.stim_bits = m->stim_bits;
     d.step_t = m->step_t;
     d.step_stim = m->step_stim;
@@ -70,7 +71,21 @@ MonoDev make_dev(const tcb_mono* m) {
     d.cm = m->cm;
     d.dt = m->dt;
     for (int k = 0; k < TCB_MAX_STIMULI; ++k) d.amp[k] = m->stim_amp[k];
+    d.wait = wait_limit();
     return d;
+}
+
+// TCB_TEST_WAIT_STALL=grid|copy makes a bounded wait run out after 10 ms (the
+// failure-detection tests); unset, the waits only guard against a lost block.
+cgk::WaitLimit wait_limit() {
+    cgk::WaitLimit w = {cgk::kBarrierTimeoutNs, 0u, 0u};
+    const char* v = getenv("TCB_TEST_WAIT_STALL");
+    if (v && (strcmp(v, "grid") == 0 || strcmp(v, "copy") == 0)) {
+        w.timeout_ns = 10000000ull;
+        w.extra_arrivals = strcmp(v, "grid") == 0 ? 1u : 0u;
+        w.drop_first_copy = strcmp(v, "copy") == 0 ? 1u : 0u;
+    }
+    return w;
 }
 
 namespace {
@@ -90,6 +105,8 @@ int validate(const tcb_mono* m) {
         return fail(TCB_EINVAL, "tcb_mono: tables not 16-byte aligned");
     if (m->max_iter < 0 || m->per_frame < 0 || m->snap_ring < 0)
         return fail(TCB_EINVAL, "tcb_mono: negative max_iter/per_frame/snap_ring");
+    if (m->ionic_variant < 0 || m->cg_per_sm < 0 || m->cg_per_sm > 2)
+        return fail(TCB_EINVAL, "tcb_mono: ionic_variant < 0 or cg_per_sm outside 0..2");
     return TCB_OK;
 }
 }  // namespace
@@ -208,7 +225,7 @@ extern "C" int tcb_mono_check(const tcb_mono* m, void* stream) {
     int32_t host[2] = {0, 0};
     TCB_CHECK_CUDA(cudaMemcpyAsync(host, m->counter, sizeof host, cudaMemcpyDeviceToHost, s));
     TCB_CHECK_CUDA(cudaStreamSynchronize(s));
-    if (host[1] == TCB_ETIMEOUT) return fail(TCB_ETIMEOUT, "a grid barrier of the CG kernel timed out");
+    if (host[1] == TCB_ETIMEOUT) return fail(TCB_ETIMEOUT, "a bounded wait (grid barrier) of the CG kernel timed out");
     if (host[1] != 0) return fail(host[1], "device error word set");
     return TCB_OK;
 }

@@ -164,6 +164,7 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
     ws.parts = reinterpret_cast<double*>(dp(L.parts));
     ws.bar = reinterpret_cast<uint32_t*>(dp(L.bar));
     ws.err = reinterpret_cast<int32_t*>(dp(L.err));
+    ws.wait = wait_limit();
     memcpy(hp(L.dev), devs.data(), sizeof(MonoDev) * n);
     memcpy(hp(L.cg), views.data(), sizeof(CgView) * n);
     memcpy(hp(L.slices), slices.data(), sizeof(int32_t) * n);
@@ -273,7 +274,7 @@ extern "C" int tcb_batch_check(const tcb_batch_plan* plan, void* stream) {
     TCB_CHECK_CUDA(cudaStreamSynchronize(s));
     int32_t err = 0;
     TCB_CHECK_CUDA(cudaMemcpy(&err, ws.err, sizeof err, cudaMemcpyDeviceToHost));
-    if (err == TCB_ETIMEOUT) return fail(TCB_ETIMEOUT, "a grid barrier of the batched CG kernel timed out");
+    if (err == TCB_ETIMEOUT) return fail(TCB_ETIMEOUT, "a bounded wait (grid barrier or bulk-copy mbarrier) of the batched CG kernel timed out");
     if (err != 0) return fail(err, "batch device error word set");
     return TCB_OK;
 }

@@ -51,6 +51,7 @@ struct BatchWS {
     double* parts;             // [3 values][n][nb] per-simulation block partials
     uint32_t* bar;             // [4] grid barrier words
     int32_t* err;              // [1] error word
+    cgk::WaitLimit wait;       // bounded-wait limits (grid barrier, bulk-copy mbarriers)
     BatchGroup groups[kBatchGroups];
 };
 

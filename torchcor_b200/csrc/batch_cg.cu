@@ -240,13 +240,13 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
     return done != 0;
 }
 
-// warp-uniform wait for a stage's copies; gives up after the barrier timeout
-// (error word set) so a lost copy can never hang the kernel
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* err) {
+// warp-uniform wait for a stage's copies; gives up after the timeout (error
+// word set) so a lost copy can never hang the kernel
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* err, const WaitLimit& w) {
     if (__all_sync(0xffffffffu, mbar_test(bar, parity))) return true;
     const uint64_t t0 = globaltimer();
     while (!__all_sync(0xffffffffu, mbar_test(bar, parity))) {
-        if (globaltimer() - t0 > kBarrierTimeoutNs) {
+        if (globaltimer() - t0 > w.timeout_ns) {
             if ((threadIdx.x & 31) == 0) atomicCAS(err, 0, TCB_ETIMEOUT);
             return false;
         }
@@ -258,8 +258,21 @@ struct Pipe {
     unsigned char* buf;   // this warp's kStages buffers of stage_bytes
     uint64_t* bar;        // their mbarriers
     uint32_t phase;       // bit s: parity of stage s's next completion
+    uint32_t inflight;    // bit s: stage s has copies issued and not yet waited for
+    uint32_t drop;        // test hook: skip the copy of the next issue (its bytes never arrive)
     int stage_bytes;
 };
+
+// After a timed-out wait: give every stage with issued copies a bounded wait of
+// its own, so that no bulk copy still writes this warp's buffers when the block
+// returns.
+__device__ __forceinline__ void drain(Pipe& P, int32_t* err, const WaitLimit& w) {
+    for (int s = 0; s < kStages; ++s)
+        if ((P.inflight >> s) & 1u) {
+            mbar_wait(P.bar + s, (P.phase >> s) & 1u, err, w);
+            P.inflight &= ~(1u << s);
+        }
+}
 
 struct Row {
     double v[3];   // per-row partial sums carried across a slice's units
@@ -487,8 +500,11 @@ __device__ __forceinline__ void issue(Pipe& P, int s, const CgView& d, const Wal
         // order this warp's earlier shared-memory reads of the stage before the async writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive_tx(P.bar + s, (uint32_t)(nk * TCB_SLICE * Streams::entry_bytes(d)));
-        Streams::copy(d, u.s0 + (int64_t)u.k0 * TCB_SLICE, nk, P.buf + (size_t)s * P.stage_bytes, P.bar + s);
+        if (!P.drop)
+            Streams::copy(d, u.s0 + (int64_t)u.k0 * TCB_SLICE, nk, P.buf + (size_t)s * P.stage_bytes, P.bar + s);
     }
+    P.drop = 0;
+    P.inflight |= 1u << s;
 }
 
 // sweep() with the ELL streams staged: unit(i, view, ls, nk, stage buffer, row)
@@ -532,10 +548,12 @@ __device__ __forceinline__ bool sweep_staged(const BatchWS* W, BatchShared& S, d
         int ci = -1;
         for (int u = 0; cons.ok && good; ++u) {
             const int st = u % kStages;
-            if (!mbar_wait(P.bar + st, (P.phase >> st) & 1u, err)) {
+            if (!mbar_wait(P.bar + st, (P.phase >> st) & 1u, err, W->wait)) {
+                drain(P, err, W->wait);
                 good = false;
                 break;
             }
+            P.inflight &= ~(1u << st);
             P.phase ^= 1u << st;
             const CgView& d = S.cg[cons.i - j0];
             if (cons.i != ci) {
@@ -749,6 +767,8 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
         P.buf = base + kStageBarBytes + (size_t)warp * kStages * stage_bytes;
         P.stage_bytes = stage_bytes;
         P.phase = 0;
+        P.inflight = 0;
+        P.drop = (W->wait.drop_first_copy && blockIdx.x == 0 && warp == 0) ? 1u : 0u;
         if (lane == 0) {
             for (int st = 0; st < kStages; ++st) mbar_init(P.bar + st);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -788,7 +808,7 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
             rhs_slice<(F & 4) != 0, (F & 2) != 0, (F & 1) != 0>(d, step, ls, lane, acc);
         });
     });
-    if (!grid_barrier(W->bar, err)) return;
+    if (!grid_barrier(W->bar, err, W->wait)) return;
     totals<2>(W, S, parts0, [&](int i, double* t) {
         S.bn[i] = sqrt(t[0]);
         S.rz[i] = t[1];
@@ -828,7 +848,7 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
                 else ap_slice<DC, false>(d, pin, pout, beta, ls, lane, acc);
             });
         });
-        if (!grid_barrier(W->bar, err)) return;
+        if (!grid_barrier(W->bar, err, W->wait)) return;
         totals<1>(W, S, parts1, [&](int i, double* t) { S.al[i] = S.rz[i] / t[0]; });
 
         // ---- x += alpha p, r -= alpha Ap, z = D r; ||z||^2, r.z
@@ -846,7 +866,7 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
             acc[0] += (double)z32 * (double)z32;
             acc[1] += (double)r32 * (double)z32;
         });
-        if (!grid_barrier(W->bar, err)) return;
+        if (!grid_barrier(W->bar, err, W->wait)) return;
         totals<2>(W, S, parts0, [&](int i, double* t) {
             const MonoDev& d = W->dev[i];
             const double zn = sqrt(t[0]);

@@ -1,6 +1,6 @@
 // Batched ionic step: one launch covers every simulation of the batch, each
-// block running the model of its group (compiled with -fmad=false, like ionic.cu; the
-// per-node work is the same ionic_node the single-simulation kernel runs).
+// block running the model of its group (the per-node work is the ionic_node the
+// single-simulation kernel runs, with the same per-step arithmetic).
 //
 // Threads walk a virtual node space made of each simulation's 128-node tiles;
 // a tile always lies in one simulation, so the simulation lookup (binary search

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
         acc2[1] += (double)r32 * z;
     }
     block_partial<2>(acc2, parts0, sh_part);
-    if (!grid_barrier(d.bar, err)) return;
+    if (!grid_barrier(d.bar, err, d.wait)) return;
     double tot[2];
     grid_total<2>(parts0, tot, sh_tot);
     const double b_norm = sqrt(tot[0]);
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
         }
         __syncthreads();
         block_partial<1>(acc1, parts1, sh_part);
-        if (!grid_barrier(d.bar, err)) return;
+        if (!grid_barrier(d.bar, err, d.wait)) return;
         double pap[1];
         grid_total<1>(parts1, pap, sh_tot);
         const double alpha = rz / pap[0];
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
         }
         __syncthreads();
         block_partial<2>(acc2, parts0, sh_part);
-        if (!grid_barrier(d.bar, err)) return;
+        if (!grid_barrier(d.bar, err, d.wait)) return;
         grid_total<2>(parts0, tot, sh_tot);
         const double zn = sqrt(tot[0]);
         if (zn < d.a_tol || (zn / b_norm) < d.r_tol) break;   // solver.py:66-69
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) cg_kernel(MonoDev d) {
             if (row >= d.n) continue;
             p[row] = (float)(beta * (double)p[row] + (double)dinv[row] * (double)r[row]);
         }
-        if (!grid_barrier(d.bar, err)) return;
+        if (!grid_barrier(d.bar, err, d.wait)) return;
         ++it;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -14,6 +14,19 @@ constexpr int kMinSlicesPerBlock = 2 * kCgWarps;
 constexpr int kMaxBlocks = 2048;
 constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;  // 2 s: a wait that long means a lost block
 
+// Limits of the bounded device waits (grid barriers, bulk-copy mbarriers).
+// In normal runs: the 2 s timeout and nothing else.  The failure-detection
+// tests set TCB_TEST_WAIT_STALL (wait_limit() in api.cu): then the timeout is
+// 10 ms and either every grid barrier waits for one arrival more than the grid
+// has ("grid") or the first bulk copy of the batched kernel's first warp is not
+// issued while its mbarrier still expects the bytes ("copy"), so that a wait
+// runs out, the error word is set and every block returns.
+struct WaitLimit {
+    uint64_t timeout_ns;
+    uint32_t extra_arrivals;
+    uint32_t drop_first_copy;
+};
+
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -34,7 +47,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Grid-wide barrier with a bounded wait: returns false (and the kernel must
 // return) if any block recorded an error or the wait ran past the timeout.
-__device__ __forceinline__ bool grid_barrier(uint32_t* bar, int32_t* err) {
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, int32_t* err, const WaitLimit& w) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -42,7 +55,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, int32_t* err) {
         const unsigned gen = ld_acquire(bar + 1);
         __threadfence();
         const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
+        if (arrived == gridDim.x - 1 + w.extra_arrivals) {
             atomicExch(bar, 0u);
             __threadfence();
             atomicAdd(bar + 1, 1u);
@@ -53,7 +66,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, int32_t* err) {
                     good = 0;
                     break;
                 }
-                if (globaltimer() - t0 > kBarrierTimeoutNs) {
+                if (globaltimer() - t0 > w.timeout_ns) {
                     atomicCAS(err, 0, TCB_ETIMEOUT);
                     good = 0;
                     break;

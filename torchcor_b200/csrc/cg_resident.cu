@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
         acc2[1] += (double)r32 * (double)z32;
     }
     block_partial<2>(acc2, parts0, sh_part);
-    if (!grid_barrier(d.bar, err)) return;
+    if (!grid_barrier(d.bar, err, d.wait)) return;
     double tot[2];
     grid_total<2>(parts0, tot, sh_tot);
     const double b_norm = sqrt(tot[0]);
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
         }
         __syncthreads();
         block_partial<1>(acc1, parts1, sh_part);
-        if (!grid_barrier(d.bar, err)) return;
+        if (!grid_barrier(d.bar, err, d.wait)) return;
         double pap[1];
         grid_total<1>(parts1, pap, sh_tot);
         const double alpha = rz / pap[0];
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kCgThreads, MINB) cg_resident_kernel(MonoDev d
         }
         __syncthreads();
         block_partial<2>(acc2, parts0, sh_part);
-        if (!grid_barrier(d.bar, err)) return;
+        if (!grid_barrier(d.bar, err, d.wait)) return;
         grid_total<2>(parts0, tot, sh_tot);
         const double zn = sqrt(tot[0]);
         if (zn < d.a_tol || (zn / b_norm) < d.r_tol) break;   // solver.py:66-69
@@ -276,9 +276,8 @@ constexpr int kResidentBytesPerRow = 6 * sizeof(float);
 // Grid of the resident kernel: the most blocks per SM (2, else 1) whose rows fit.
 bool resident_plan(const MonoDev& d, unsigned* nb_out, int* cap_out, size_t* smem_out, int* per_sm_out, bool int16) {
     ResidentInfo& ri = resident_info();
-    // TCB_CG_PER_SM=1|2 pins the blocks per SM (tuning); default: 2 if the rows fit, else 1
-    const char* env = getenv("TCB_CG_PER_SM");
-    const int hi = env && env[0] == '1' ? 1 : 2, lo = env && env[0] == '2' ? 2 : 1;
+    // d.cg_per_sm = 1 or 2 pins the blocks per SM (a tuning choice); 0: 2 if the rows fit, else 1
+    const int hi = d.cg_per_sm == 1 ? 1 : 2, lo = d.cg_per_sm == 2 ? 2 : 1;
     for (int per_sm = hi; per_sm >= lo; --per_sm) {
         int64_t want = ceil_div(d.n_slices, kMinSlicesPerBlock);
         int64_t nb = std::min<int64_t>(want, (int64_t)ri.sms * per_sm);

@@ -1,11 +1,17 @@
-// Ionic-model kernels: lookup-table construction, initial state,
-// stand-alone differentiate(), and the fused per-step kernel of the
-// monodomain loop (activation/repolarisation update of the previous step,
-// snapshot, ionic update, stimulus injection and the right-hand side
-// b' = u*Cm + dt*du/100 + dt*Istim/100 of monodomain.py:117-128).
+// Per-step ionic kernels: the stand-alone differentiate() and the fused
+// per-step kernel of the monodomain loop (activation/repolarisation update of
+// the previous step, snapshot, ionic update, stimulus injection and the
+// right-hand side b' = u*Cm + dt*du/100 + dt*Istim/100 of monodomain.py:117-128).
 //
-// Compiled with -fmad=false: every float32 operation rounds separately, as
-// the reference's element-wise tensor ops do.
+// The fused kernel is instantiated for several launch shapes: 1, 2 or 4
+// consecutive nodes per thread (structure-of-arrays state read and written as
+// 4-, 8- or 16-byte vectors) and a register budget set by the blocks per SM it
+// is compiled for.  tcb_mono.ionic_variant picks one (the autotuner measures
+// them); every instance runs the same per-node arithmetic.
+//
+// Compiled with multiply-add contraction; the per-step division and logarithm
+// are the hardware forms (ionic_common.cuh).  Lookup tables are built in
+// tables.cu with separate roundings.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -19,19 +25,6 @@
 
 namespace tcb {
 
-int64_t LutSpec::rows() const { return (int64_t)ceil((mx - mn) / res); }
-int32_t LutSpec::mx_idx() const { return (int32_t)((mx - mn) * (1.0 / res)) - 1; }
-Lut LutSpec::make(const float* tab) const {
-    Lut L;
-    L.tab = tab;
-    L.mn = (float)mn;
-    L.mx = (float)mx;
-    L.res = (float)res;
-    L.step = (float)(1.0 / res);
-    L.mx_idx = mx_idx();
-    return L;
-}
-
 namespace {
 
 constexpr int kThreads = 256;
@@ -39,85 +32,6 @@ constexpr int kThreads = 256;
 inline unsigned grid_for(int64_t n) {
     int64_t b = ceil_div(n, kThreads);
     return (unsigned)(b > 148 * 64 ? 148 * 64 : b);
-}
-
-// ------------------------------------------------------------- tables
-// Grid value of row i of a table built on torch.arange(mn, mx, res) in
-// float32 on the CPU, as PyTorch's CPU kernel forms it: the range is split
-// into chunks of max(32768, ceil(rows/8)) (its parallel grain on the 8-thread
-// host the reference fixtures come from); inside a chunk, whole 16-element
-// groups are vectorised as 8-wide vectors whose first element is
-// float(fma(res, i0, mn)) and whose element k is float(fma(k, res, first));
-// the remaining elements take float(fma(res, i, mn)).  The exact grid matters
-// at removable singularities of the table formulas (e.g. V = 7.9 in CRN tau_w).
-__device__ inline float grid_value(double mn, double res, int64_t i, int64_t rows) {
-    const int64_t chunk = rows / 8 + (rows % 8 != 0) > 32768 ? rows / 8 + (rows % 8 != 0) : 32768;
-    const int64_t cb = (i / chunk) * chunk;
-    const int64_t ce = cb + chunk < rows ? cb + chunk : rows;
-    const int64_t vec_end = cb + ((ce - cb) / 16) * 16;
-    if (i < vec_end) {
-        const int64_t i0 = cb + ((i - cb) / 8) * 8;
-        const float base = (float)__fma_rn(res, (double)i0, mn);
-        return (float)__fma_rn((double)(i - i0), res, (double)base);
-    }
-    return (float)__fma_rn(res, (double)i, mn);
-}
-
-__global__ void ttp_v_table(TTP::C c, float* tab, int64_t rows, double mn, double res) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-        float o[TV_NCOL];
-        TTP::v_row(grid_value(mn, res, i, rows), c, o);
-        constexpr int S = lut_stride(TV_NCOL);
-        for (int k = 0; k < S; ++k) tab[i * S + k] = k < TV_NCOL ? o[k] : 0.0f;
-    }
-}
-__global__ void ttp_cass_table(TTP::C c, float* tab, int64_t rows, double mn, double res) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-        float o[3];
-        TTP::cass_row(grid_value(mn, res, i, rows), c, o);
-        constexpr int S = lut_stride(3);
-        for (int k = 0; k < S; ++k) tab[i * S + k] = k < 3 ? o[k] : 0.0f;
-    }
-}
-__global__ void ttp_vek_table(float* tab, int64_t rows, double mn, double res) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x)
-        tab[i] = TTP::vek_row(grid_value(mn, res, i, rows));
-}
-__global__ void crn_v_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-        float o[CV_NCOL];
-        CRN::v_row(grid_value(mn, res, i, rows), c, o);
-        constexpr int S = lut_stride(CV_NCOL);
-        for (int k = 0; k < S; ++k) tab[i * S + k] = k < CV_NCOL ? o[k] : 0.0f;
-    }
-}
-__global__ void crn_cai_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-        float o[CC_NCOL];
-        CRN::cai_row(grid_value(mn, res, i, rows), c, o);
-        constexpr int S = lut_stride(CC_NCOL);
-        for (int k = 0; k < S; ++k) tab[i * S + k] = k < CC_NCOL ? o[k] : 0.0f;
-    }
-}
-__global__ void crn_fn_table(CRN::C c, float* tab, int64_t rows, double mn, double res) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-        float o[3];
-        CRN::fn_row(grid_value(mn, res, i, rows), c, o);
-        constexpr int S = lut_stride(3);
-        for (int k = 0; k < S; ++k) tab[i * S + k] = k < 3 ? o[k] : 0.0f;
-    }
-}
-
-// ------------------------------------------------------------- init / differentiate
-template <class M>
-__global__ void init_kernel(typename M::C c, float* state, int64_t n_pad, float* v) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += (int64_t)gridDim.x * blockDim.x) {
-        float s[M::kStates];
-        float V;
-        M::init(c, s, V);
-        for (int k = 0; k < M::kStates; ++k) state[k * n_pad + i] = s[k];
-        if (v) v[i] = V;
-    }
 }
 
 template <class M>
@@ -134,11 +48,12 @@ __global__ void differentiate_kernel(typename M::C c, typename M::Tables T, floa
     }
 }
 
-template <class M>
-__global__ void __launch_bounds__(kThreads, M::kMinBlocksPerSm) mono_ionic_kernel(MonoDev d, typename M::C c, typename M::Tables T) {
+template <class M, int V, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) mono_ionic_kernel(MonoDev d, typename M::C c, typename M::Tables T) {
     const StepView sv = step_view(d, d.counter[0]);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += (int64_t)gridDim.x * blockDim.x)
-        ionic_node<M>(d, c, T, sv, i);
+    const int64_t groups = (d.n + V - 1) / V;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (int64_t)gridDim.x * blockDim.x)
+        ionic_group<M, V>(d, c, T, sv, g * V);
 }
 
 __global__ void mono_finish_kernel(MonoDev d) {
@@ -157,19 +72,61 @@ __global__ void mono_finish_kernel(MonoDev d) {
 }
 
 template <class M>
-int launch_mono(const tcb_mono* m, const MonoDev& d, cudaStream_t s) {
-    typename M::C c = M::derive(m->params);
-    typename M::Tables T = M::tables(m->tables, m->params);
-    mono_ionic_kernel<M><<<grid_for(d.n), kThreads, 0, s>>>(d, c, T);
+using LaunchFn = int (*)(const MonoDev&, const typename M::C&, const typename M::Tables&, cudaStream_t);
+
+template <class M, int V, int MINB>
+int launch_shape(const MonoDev& d, const typename M::C& c, const typename M::Tables& T, cudaStream_t s) {
+    mono_ionic_kernel<M, V, MINB><<<grid_for(ceil_div(d.n, V)), kThreads, 0, s>>>(d, c, T);
     TCB_CHECK_LAUNCH("mono ionic kernel");
     return TCB_OK;
 }
 
+// The instances of each model (nodes per thread, 256-thread blocks per SM the
+// register budget is set for); entry 0 is the default.
+struct Shape {
+    int32_t nodes_per_thread, blocks_per_sm;
+};
 template <class M>
-int run_init(const double* params, float* state, int64_t n_pad, float* v, cudaStream_t s) {
-    init_kernel<M><<<grid_for(n_pad), kThreads, 0, s>>>(M::derive(params), state, n_pad, v);
-    TCB_CHECK_LAUNCH("init kernel");
-    return TCB_OK;
+struct Shapes;
+template <>
+struct Shapes<MS> {
+    static constexpr int kCount = 3;
+    static constexpr Shape shape[kCount] = {{1, 1}, {2, 1}, {4, 1}};
+    static constexpr LaunchFn<MS> fn[kCount] = {launch_shape<MS, 1, 1>, launch_shape<MS, 2, 1>, launch_shape<MS, 4, 1>};
+};
+template <>
+struct Shapes<TTP> {
+    static constexpr int kCount = 6;
+    static constexpr Shape shape[kCount] = {{1, 6}, {1, 4}, {2, 4}, {2, 3}, {4, 3}, {4, 2}};
+    static constexpr LaunchFn<TTP> fn[kCount] = {launch_shape<TTP, 1, 6>, launch_shape<TTP, 1, 4>,
+                                                 launch_shape<TTP, 2, 4>, launch_shape<TTP, 2, 3>,
+                                                 launch_shape<TTP, 4, 3>, launch_shape<TTP, 4, 2>};
+};
+template <>
+struct Shapes<CRN> {
+    static constexpr int kCount = 4;
+    static constexpr Shape shape[kCount] = {{1, 3}, {1, 2}, {2, 2}, {4, 1}};
+    static constexpr LaunchFn<CRN> fn[kCount] = {launch_shape<CRN, 1, 3>, launch_shape<CRN, 1, 2>,
+                                                 launch_shape<CRN, 2, 2>, launch_shape<CRN, 4, 1>};
+};
+
+inline bool aligned(const void* p, unsigned bytes) { return ((uintptr_t)p & (bytes - 1)) == 0; }
+
+// Vector accesses need every per-node array aligned to the vector: otherwise the
+// first one-node-per-thread instance runs.
+template <class M>
+int launch_mono(const tcb_mono* m, const MonoDev& d, cudaStream_t s) {
+    typename M::C c = M::derive(m->params);
+    typename M::Tables T = M::tables(m->tables, m->params);
+    int k = m->ionic_variant > 0 ? m->ionic_variant - 1 : 0;
+    if (k >= Shapes<M>::kCount) return fail(TCB_ERANGE, "tcb_mono: no such ionic kernel variant");
+    const unsigned vb = 4u * (unsigned)Shapes<M>::shape[k].nodes_per_thread;
+    if (vb > 4 && !(aligned(d.x, vb) && aligned(d.state, vb) && aligned(d.bp, vb) && aligned(d.at, vb) &&
+                    aligned(d.rt, vb) && aligned(d.stim_bits, vb))) {
+        k = 0;
+        while (Shapes<M>::shape[k].nodes_per_thread != 1) ++k;
+    }
+    return Shapes<M>::fn[k](d, c, T, s);
 }
 
 template <class M>
@@ -192,6 +149,16 @@ int launch_mono_ionic(const tcb_mono* m, const MonoDev& d, cudaStream_t s) {
     return fail(TCB_EINVAL, "unknown ionic model");
 }
 
+template <class M>
+int variant_info(int32_t variant, int32_t* count, int32_t* nodes_per_thread, int32_t* blocks_per_sm) {
+    *count = Shapes<M>::kCount;
+    if (variant < 0 || variant > Shapes<M>::kCount) return fail(TCB_ERANGE, "no such ionic kernel variant");
+    const Shape& sh = Shapes<M>::shape[variant > 0 ? variant - 1 : 0];
+    *nodes_per_thread = sh.nodes_per_thread;
+    *blocks_per_sm = sh.blocks_per_sm;
+    return TCB_OK;
+}
+
 int launch_mono_finish(const MonoDev& d, cudaStream_t s) {
     mono_finish_kernel<<<grid_for(d.n), kThreads, 0, s>>>(d);
     TCB_CHECK_LAUNCH("mono finish kernel");
@@ -201,114 +168,6 @@ int launch_mono_finish(const MonoDev& d, cudaStream_t s) {
 }  // namespace tcb
 
 using namespace tcb;
-
-extern "C" const char* tcb_model_params(int32_t model) {
-    switch (model) {
-        case TCB_MODEL_MS: return TCB_MS_PARAMS;
-        case TCB_MODEL_TTP: return TCB_TTP_PARAMS;
-        case TCB_MODEL_CRN: return TCB_CRN_PARAMS;
-    }
-    return nullptr;
-}
-
-extern "C" const char* tcb_model_states(int32_t model) {
-    switch (model) {
-        case TCB_MODEL_MS: return TCB_MS_STATES;
-        case TCB_MODEL_TTP: return TCB_TTP_STATES;
-        case TCB_MODEL_CRN: return TCB_CRN_STATES;
-    }
-    return nullptr;
-}
-
-extern "C" int tcb_model_layout(int32_t model, const double* params, int64_t* n_states, int64_t* table_floats) {
-    if (!n_states || !table_floats) return fail(TCB_EINVAL, "tcb_model_layout: null output");
-    switch (model) {
-        case TCB_MODEL_MS:
-            *n_states = MS::kStates;
-            *table_floats = MS::table_floats(params);
-            return TCB_OK;
-        case TCB_MODEL_TTP:
-            *n_states = TTP::kStates;
-            *table_floats = TTP::table_floats(params);
-            return TCB_OK;
-        case TCB_MODEL_CRN:
-            *n_states = CRN::kStates;
-            *table_floats = CRN::table_floats(params);
-            return TCB_OK;
-    }
-    return fail(TCB_EINVAL, "unknown ionic model");
-}
-
-extern "C" int tcb_model_table_info(int32_t model, int32_t index, int64_t* rows, int32_t* ncol, int32_t* stride,
-                                    int64_t* offset) {
-    if (!rows || !ncol || !stride || !offset) return fail(TCB_EINVAL, "tcb_model_table_info: null output");
-    const LutSpec* specs[3] = {nullptr, nullptr, nullptr};
-    if (model == TCB_MODEL_TTP) {
-        specs[0] = &TTP::kV;
-        specs[1] = &TTP::kCaSS;
-        specs[2] = &TTP::kVEk;
-    } else if (model == TCB_MODEL_CRN) {
-        specs[0] = &CRN::kV;
-        specs[1] = &CRN::kCai;
-        specs[2] = &CRN::kFn;
-    } else if (model != TCB_MODEL_MS) {
-        return fail(TCB_EINVAL, "unknown ionic model");
-    }
-    if (index < 0 || index > 2 || !specs[index]) return fail(TCB_ERANGE, "no such lookup table");
-    int64_t off = 0;
-    for (int i = 0; i < index; ++i) off += specs[i]->floats();
-    *rows = specs[index]->rows();
-    *ncol = specs[index]->ncol;
-    *stride = specs[index]->stride();
-    *offset = off;
-    return TCB_OK;
-}
-
-extern "C" int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream) {
-    if (!params) return fail(TCB_EINVAL, "tcb_model_tables: null params");
-    cudaStream_t s = as_stream(stream);
-    if (model == TCB_MODEL_MS) return TCB_OK;
-    if (!tables) return fail(TCB_EINVAL, "tcb_model_tables: null tables");
-    if ((uintptr_t)tables & 15u) return fail(TCB_EINVAL, "tcb_model_tables: tables not 16-byte aligned");
-    if (model == TCB_MODEL_TTP) {
-        TTP::C c = TTP::derive(params);
-        TTP::Tables T = TTP::tables(tables, params);
-        ttp_v_table<<<grid_for(TTP::kV.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.V.tab), TTP::kV.rows(),
-                                                                    TTP::kV.mn, TTP::kV.res);
-        ttp_cass_table<<<grid_for(TTP::kCaSS.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.CaSS.tab),
-                                                                          TTP::kCaSS.rows(), TTP::kCaSS.mn,
-                                                                          TTP::kCaSS.res);
-        ttp_vek_table<<<grid_for(TTP::kVEk.rows()), kThreads, 0, s>>>(const_cast<float*>(T.VEk.tab),
-                                                                        TTP::kVEk.rows(), TTP::kVEk.mn, TTP::kVEk.res);
-        TCB_CHECK_LAUNCH("TTP table kernels");
-        return TCB_OK;
-    }
-    if (model == TCB_MODEL_CRN) {
-        CRN::C c = CRN::derive(params);
-        CRN::Tables T = CRN::tables(tables, params);
-        crn_v_table<<<grid_for(CRN::kV.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.V.tab), CRN::kV.rows(),
-                                                                    CRN::kV.mn, CRN::kV.res);
-        crn_cai_table<<<grid_for(CRN::kCai.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.Cai.tab),
-                                                                        CRN::kCai.rows(), CRN::kCai.mn, CRN::kCai.res);
-        crn_fn_table<<<grid_for(CRN::kFn.rows()), kThreads, 0, s>>>(c, const_cast<float*>(T.Fn.tab), CRN::kFn.rows(),
-                                                                      CRN::kFn.mn, CRN::kFn.res);
-        TCB_CHECK_LAUNCH("CRN table kernels");
-        return TCB_OK;
-    }
-    return fail(TCB_EINVAL, "unknown ionic model");
-}
-
-extern "C" int tcb_model_init(int32_t model, const double* params, float* state, int64_t n_pad, float* v,
-                              void* stream) {
-    if (!params || !state || n_pad <= 0) return fail(TCB_EINVAL, "tcb_model_init: bad arguments");
-    cudaStream_t s = as_stream(stream);
-    switch (model) {
-        case TCB_MODEL_MS: return run_init<MS>(params, state, n_pad, v, s);
-        case TCB_MODEL_TTP: return run_init<TTP>(params, state, n_pad, v, s);
-        case TCB_MODEL_CRN: return run_init<CRN>(params, state, n_pad, v, s);
-    }
-    return fail(TCB_EINVAL, "unknown ionic model");
-}
 
 extern "C" int tcb_model_differentiate(int32_t model, const double* params, const float* tables, float* state,
                                        int64_t n_pad, int64_t n, const float* v, float* dv, void* stream) {
@@ -321,6 +180,17 @@ extern "C" int tcb_model_differentiate(int32_t model, const double* params, cons
         case TCB_MODEL_MS: return run_differentiate<MS>(params, tables, state, n_pad, n, v, dv, s);
         case TCB_MODEL_TTP: return run_differentiate<TTP>(params, tables, state, n_pad, n, v, dv, s);
         case TCB_MODEL_CRN: return run_differentiate<CRN>(params, tables, state, n_pad, n, v, dv, s);
+    }
+    return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+extern "C" int tcb_ionic_variant(int32_t model, int32_t variant, int32_t* count, int32_t* nodes_per_thread,
+                                 int32_t* blocks_per_sm) {
+    if (!count || !nodes_per_thread || !blocks_per_sm) return fail(TCB_EINVAL, "tcb_ionic_variant: null output");
+    switch (model) {
+        case TCB_MODEL_MS: return variant_info<MS>(variant, count, nodes_per_thread, blocks_per_sm);
+        case TCB_MODEL_TTP: return variant_info<TTP>(variant, count, nodes_per_thread, blocks_per_sm);
+        case TCB_MODEL_CRN: return variant_info<CRN>(variant, count, nodes_per_thread, blocks_per_sm);
     }
     return fail(TCB_EINVAL, "unknown ionic model");
 }

@@ -1,12 +1,18 @@
 // Arithmetic helpers shared by the ionic-model kernels.
 //
-// The kernels reproduce the float32 operation order of the reference's
-// PyTorch expressions (the ionic translation units are compiled with
-// -fmad=false so a*b+c stays two roundings, as in separate tensor ops):
+// Two fidelity levels.  The lookup tables (built once per simulation; tables.cu,
+// compiled with -fmad=false) reproduce the float32 operation order of the
+// reference's PyTorch expressions with separate roundings:
 //  * a Python float meeting a float32 tensor is rounded to float32 first;
 //  * `python_float / tensor` is evaluated by PyTorch as
 //    `tensor.reciprocal() * python_float` -> sdiv() below;
 //  * `tensor / python_float` is a true division by the rounded float.
+// Their grids pass through removable singularities where the last ulp decides
+// between a finite value and NaN, so they keep IEEE division.
+// The per-step updates (every node, every step) keep the reference's order of
+// operations but let the compiler fuse multiply-adds and use the hardware
+// division and logarithm (qdiv, qsdiv, qlog): a few ulp per operation, far
+// inside the 1e-3 membrane-potential tolerance, for fewer instructions.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -26,6 +32,28 @@ constexpr int count_names(const char* s) {
 
 // python_float / tensor
 TCB_HD float sdiv(float s, float t) { return (1.0f / t) * s; }
+
+// a / b in a per-step update: __fdividef (a times the hardware reciprocal of b,
+// within 2 ulp for |b| below 2^126; every denominator here is far smaller)
+TCB_HD float qdiv(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+// python_float / tensor in a per-step update (reciprocal then product, as sdiv)
+TCB_HD float qsdiv(float s, float t) { return qdiv(s, t); }
+// natural logarithm in a per-step update (__logf: absolute error below 2^-21.4
+// on [0.5, 2], a few ulp elsewhere; the arguments here are positive
+// concentration ratios)
+TCB_HD float qlog(float x) {
+#ifdef __CUDA_ARCH__
+    return __logf(x);
+#else
+    return logf(x);
+#endif
+}
 
 // torch.clamp(X, mn, mx) with NaN propagation
 TCB_HD float tclamp(float x, float mn, float mx) {
@@ -53,7 +81,7 @@ TCB_HD LutPos lut_pos(float X, const Lut& L) {
     idx = idx < 0 ? 0 : idx;
     idx = idx > L.mx_idx - 1 ? L.mx_idx - 1 : idx;
     float lo_pos = (float)idx * L.res + L.mn;
-    float w = (X - lo_pos) / L.res;
+    float w = qdiv(X - lo_pos, L.res);
     LutPos p;
     p.lo = (int32_t)idx;
     p.w = w;

@@ -37,10 +37,6 @@ enum CRNS { R_Ca_rel, R_Ca_up, R_Cai, R_Ki, R_d, R_f, R_f_Ca, R_h, R_j, R_m, R_o
 
 struct CRN {
     static constexpr int kStates = CRN_NS;
-    // 256-thread blocks per SM the single-simulation ionic kernel is compiled for: 3
-    // (80 registers, 60 bytes of spills) against 1 unbounded (218 registers): 0.059 ->
-    // 0.033 ms a launch on a 531,441-node cube on B200; 2 and 4 measured slower
-    static constexpr int kMinBlocksPerSm = 3;
     static constexpr LutSpec kCai{3e-4, 30.0, 3e-4, CC_NCOL};
     static constexpr LutSpec kV{-200.0, 200.0, 0.1, CV_NCOL};
     static constexpr LutSpec kFn{-2e-11, 10.0e-11, 2e-15, 3};
@@ -269,23 +265,25 @@ struct CRN {
     }
 
     // ------------------------------------------------ differentiate (:358-444)
+    // The reference's order of operations with the per-step division and
+    // logarithm (qdiv, qsdiv, qlog; ionic_common.cuh).
     __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
         LutPos pv = lut_pos(V, T.V);
         LutPos pc = lut_pos(s[R_Cai], T.Cai);
 #define VR(col) lut_col<CV_NCOL>(T.V, pv, col)
 #define CR(col) lut_col<CC_NCOL>(T.Cai, pc, col)
-        float E_K = c.RTF * logf(sdiv(c.Ko, s[R_Ki]));
+        float E_K = c.RTF * qlog(qsdiv(c.Ko, s[R_Ki]));
         float VmK = V - E_K;
         float ICaL = ((VR(CV_vrow_29) * s[R_d]) * s[R_f]) * s[R_f_Ca];
-        float IKACh = (c.ACh_term * (sdiv(0.4516f, 1.0f + expf((V + 59.53f) / 17.18f)) + 0.0517f)) * VmK;
+        float IKACh = (c.ACh_term * (qsdiv(0.4516f, 1.0f + expf(qdiv(V + 59.53f, 17.18f))) + 0.0517f)) * VmK;
         float m = s[R_m];
         float INa = ((((VR(CV_vrow_7) * m) * m) * m) * s[R_h]) * s[R_j];
         float INaCa = VR(CV_vrow_31) - (s[R_Cai] * VR(CV_vrow_32));
         float vrow_13 = c.Gto * VmK;
         float vrow_18 = (c.factorGKur * VR(CV_GKur)) * VmK;
-        float vrow_21 = (c.GKr * VmK) / (1.0f + expf((V + 15.0f) / 22.4f));
+        float vrow_21 = qdiv(c.GKr * VmK, 1.0f + expf(qdiv(V + 15.0f, 22.4f)));
         float vrow_24 = c.GKs * VmK;
-        float IK1 = (c.GK1 * VmK) / (1.0f + expf(0.07f * (V + 80.0f)));
+        float IK1 = qdiv(c.GK1 * VmK, 1.0f + expf(0.07f * (V + 80.0f)));
         float IKr = vrow_21 * s[R_xr];
         float IKs = (vrow_24 * s[R_xs]) * s[R_xs];
         float ua = s[R_ua], oa = s[R_oa];
@@ -296,14 +294,14 @@ struct CRN {
         float Iion = INa + IK1 + Ito + IKur + IKr + IKs + ICaL + IpCa + INaCa + VR(CV_IbNa) + INaK + IKACh;
 
         float Ca_rel = s[R_Ca_rel], Ca_up = s[R_Ca_up], u = s[R_u];
-        float Itr = (c.factorGtr * (Ca_up - Ca_rel)) / c.tau_tr;
+        float Itr = qdiv(c.factorGtr * (Ca_up - Ca_rel), c.tau_tr);
         float Irel = (((((c.factorGrel * u) * u) * s[R_v]) * c.k_rel) * s[R_w]) * (Ca_rel - CR(CC_conCa));
         float dIups = CR(CC_carow_1) - (c.maxIup_maxCaup * Ca_up);
         float cs = Ca_rel + c.KmCsqn;
-        float diff_Ca_rel = (Itr - Irel) / (1.0f + (sdiv(c.C_dCa_rel, cs) / cs));
-        float diff_Ki = (-((((((Ito + IKr) + IKur) + IKs) + IK1) + IKACh) - (2.0f * INaK))) / c.FVoli;
+        float diff_Ca_rel = qdiv(Itr - Irel, 1.0f + qdiv(qsdiv(c.C_dCa_rel, cs), cs));
+        float diff_Ki = qdiv(-((((((Ito + IKr) + IKur) + IKs) + IK1) + IKACh) - (2.0f * INaK)), c.FVoli);
         float diff_Ca_up = dIups - (Itr * c.C_dCaup);
-        float diff_Cai = (((c.C_B1d * (((INaCa + INaCa) - IpCa) - ICaL)) - (c.C_B1e * dIups)) + Irel) / CR(CC_carow_2);
+        float diff_Cai = qdiv(((c.C_B1d * (((INaCa + INaCa) - IpCa) - ICaL)) - (c.C_B1e * dIups)) + Irel, CR(CC_carow_2));
         s[R_Ca_rel] = Ca_rel + diff_Ca_rel * c.dt;
         s[R_Ca_up] = Ca_up + diff_Ca_up * c.dt;
         float fCaA = CR(CC_f_Ca_A);

@@ -16,7 +16,6 @@ static_assert(sizeof(MSRaw) == count_names(TCB_MS_PARAMS) * sizeof(double), "MSR
 
 struct MS {
     static constexpr int kStates = 1;
-    static constexpr int kMinBlocksPerSm = 1;
     struct C {
         float tau_in, tau_out, tau_open, tau_close, u_gate, u_crit, vmin, DV, dt, H_init, V_init;
     };

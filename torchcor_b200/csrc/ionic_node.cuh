@@ -1,5 +1,5 @@
 // Per-node work of the fused monodomain ionic step, shared by the
-// single-simulation and batched kernels (both compiled with -fmad=false).
+// single-simulation and batched kernels.
 #pragma once
 #include "ionic_common.cuh"
 #include "mono.cuh"
@@ -39,6 +39,20 @@ __device__ __forceinline__ StepView step_view(const MonoDev& d, int64_t n) {
     return v;
 }
 
+// Istim = sum of the active stimuli of a node in list order (stimulation.py:59-61)
+__device__ __forceinline__ float stim_sum(const MonoDev& d, uint32_t smask, uint32_t bits) {
+    float I = 0.0f;
+    bool first = true;
+    for (int k = 0; k < TCB_MAX_STIMULI; ++k) {
+        if ((smask >> k) & 1u) {
+            const float a = ((bits >> k) & 1u) ? d.amp[k] : 0.0f;
+            I = first ? a : I + a;
+            first = false;
+        }
+    }
+    return I;
+}
+
 // AT/RT and snapshot of the previous step, ionic update, stimulus and
 // b' = u*Cm + dt*du/100 + dt*Istim/100 (monodomain.py:117-128) for node i.
 template <class M>
@@ -54,24 +68,99 @@ __device__ __forceinline__ void ionic_node(const MonoDev& d, const typename M::C
 #pragma unroll
     for (int k = 0; k < M::kStates; ++k) d.state[k * d.n_pad + i] = s[k];
     // b = u*Cm + dt*du, du = dV/100  (monodomain.py:117-118)
-    float b = v * d.cm + d.dt * (dV / 100.0f);
+    float b = v * d.cm + d.dt * qdiv(dV, 100.0f);
     if (sv.smask) {
-        // Istim = sum of the active stimuli in list order (stimulation.py:59-61), /100 (:127)
+        // Istim/100 (monodomain.py:127), b += dt*Istim (:128)
         const uint32_t bits = d.stim_bits[i] & sv.smask;
-        if (bits) {
-            float I = 0.0f;
-            bool first = true;
-            for (int k = 0; k < TCB_MAX_STIMULI; ++k) {
-                if ((sv.smask >> k) & 1u) {
-                    const float a = ((bits >> k) & 1u) ? d.amp[k] : 0.0f;
-                    I = first ? a : I + a;
-                    first = false;
-                }
-            }
-            b = b + d.dt * (I / 100.0f);
-        }
+        if (bits) b = b + d.dt * qdiv(stim_sum(d, sv.smask, bits), 100.0f);
     }
     d.bp[i] = b;
+}
+
+// V consecutive per-node values as one 8- or 16-byte access (the arrays are
+// n_pad long, n_pad a multiple of 128, and aligned to the vector).
+template <int V, typename T>
+__device__ __forceinline__ void ld_nodes(const T* __restrict__ p, T (&o)[V]) {
+    static_assert(sizeof(T) == 4 && (V == 2 || V == 4), "2 or 4 four-byte values");
+    if constexpr (V == 4) {
+        const uint4 t = *reinterpret_cast<const uint4*>(p);
+        const uint32_t w[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) o[j] = __builtin_bit_cast(T, w[j]);
+    } else {
+        const uint2 t = *reinterpret_cast<const uint2*>(p);
+        o[0] = __builtin_bit_cast(T, t.x);
+        o[1] = __builtin_bit_cast(T, t.y);
+    }
+}
+
+template <int V>
+__device__ __forceinline__ void st_nodes(float* __restrict__ p, const float (&v)[V]) {
+    static_assert(V == 2 || V == 4, "2 or 4 floats");
+    if constexpr (V == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    else *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+}
+
+// ionic_node for the V consecutive nodes i0 .. i0+V-1 (V = 1, 2 or 4), with the
+// per-node arrays moved as vectors for V > 1.  Nodes between n and n_pad are
+// padding: their ionic arithmetic runs on memory that exists but nothing reads
+// its results; their u stays 0, so AT/RT are never set for them, and snapshots
+// are written for real nodes only.
+template <class M, int V>
+__device__ __forceinline__ void ionic_group(const MonoDev& d, const typename M::C& c, const typename M::Tables& T,
+                                            const StepView& sv, int64_t i0) {
+    if constexpr (V == 1) {
+        ionic_node<M>(d, c, T, sv, i0);
+    } else {
+        float v[V];
+        ld_nodes<V>(sv.u + i0, v);
+        if (sv.do_atrt) {
+            float a[V], r[V];
+            ld_nodes<V>(d.at + i0, a);
+            ld_nodes<V>(d.rt + i0, r);
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                if (v[j] > 0.0f && a[j] == -1.0f) {
+                    a[j] = sv.t_prev;
+                    d.at[i0 + j] = a[j];
+                }
+                if (a[j] > 0.0f && v[j] < -70.0f && r[j] == -1.0f) d.rt[i0 + j] = sv.t_prev;
+            }
+        }
+        if (sv.snap) {
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+                if (i0 + j < d.n) sv.snap[i0 + j] = v[j];
+        }
+        float s[V][M::kStates];
+#pragma unroll
+        for (int k = 0; k < M::kStates; ++k) {
+            float t[V];
+            ld_nodes<V>(d.state + k * d.n_pad + i0, t);
+#pragma unroll
+            for (int j = 0; j < V; ++j) s[j][k] = t[j];
+        }
+        float b[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) b[j] = v[j] * d.cm + d.dt * qdiv(M::step(v[j], s[j], c, T), 100.0f);
+#pragma unroll
+        for (int k = 0; k < M::kStates; ++k) {
+            float t[V];
+#pragma unroll
+            for (int j = 0; j < V; ++j) t[j] = s[j][k];
+            st_nodes<V>(d.state + k * d.n_pad + i0, t);
+        }
+        if (sv.smask) {
+            uint32_t bits[V];
+            ld_nodes<V>(d.stim_bits + i0, bits);
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                const uint32_t on = bits[j] & sv.smask;
+                if (on) b[j] = b[j] + d.dt * qdiv(stim_sum(d, sv.smask, on), 100.0f);
+            }
+        }
+        st_nodes<V>(d.bp + i0, b);
+    }
 }
 
 }  // namespace tcb

@@ -45,10 +45,6 @@ enum TTPS { S_CaSR, S_CaSS, S_Cai, S_D, S_F, S_F2, S_FCaSS, S_H, S_J, S_Ki, S_M,
 
 struct TTP {
     static constexpr int kStates = TTP_NS;
-    // 256-thread blocks per SM the single-simulation ionic kernel is compiled for: 6
-    // (40 registers, 76 bytes of spills) beats 4 (64 registers, none) by 1 % on B200;
-    // 5 measured slower
-    static constexpr int kMinBlocksPerSm = 6;
     static constexpr LutSpec kV{-800.0, 800.0, 0.05, TV_NCOL};
     static constexpr LutSpec kCaSS{0.00001, 10.0, 0.00001, 3};
     static constexpr LutSpec kVEk{-800.0, 800.0, 0.05, 1};
@@ -277,17 +273,19 @@ struct TTP {
     }
 
     // ---------------------------------------------------- differentiate (:353-454)
+    // The reference's order of operations with the per-step division and
+    // logarithm (qdiv, qsdiv, qlog; ionic_common.cuh).
     __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
         LutPos pv = lut_pos(V, T.V);
         const float CaSR = s[S_CaSR], CaSS = s[S_CaSS], Cai = s[S_Cai], Ki = s[S_Ki], Nai = s[S_Nai];
         LutPos pc = lut_pos(CaSS, T.CaSS);
-        float Eca = c.halfRTONF * logf(sdiv(c.Cao, Cai));
-        float Ek = c.RTONF * logf(sdiv(c.Ko, Ki));
-        float Eks = c.RTONF * logf(sdiv(c.KoNa, Ki + (c.pKNa * Nai)));
-        float Ena = c.RTONF * logf(sdiv(c.Nao, Nai));
-        float IpCa = (c.GpCa * Cai) / (Cai + c.KpCa);
+        float Eca = c.halfRTONF * qlog(qsdiv(c.Cao, Cai));
+        float Ek = c.RTONF * qlog(qsdiv(c.Ko, Ki));
+        float Eks = c.RTONF * qlog(qsdiv(c.KoNa, Ki + (c.pKNa * Nai)));
+        float Ena = c.RTONF * qlog(qsdiv(c.Nao, Nai));
+        float IpCa = qdiv(c.GpCa * Cai, Cai + c.KpCa);
         float v15 = V - 15.0f;
-        float a1 = c.ga1 * ((V == 15.0f) ? c.halfFRT : v15 / expm1f((2.0f * v15) * c.F_RT));
+        float a1 = c.ga1 * ((V == 15.0f) ? c.halfFRT : qdiv(v15, expm1f((2.0f * v15) * c.F_RT)));
         const float2 a2_iNaK = lut_pair<TV_NCOL>(T.V, pv, TV_a2);  // TV_a2, TV_rec_iNaK
         float ICaL_A = a1 * a2_iNaK.x;
         float ICaL_B = a1 * c.Cao;
@@ -296,7 +294,7 @@ struct TTP {
         float IKs = ((c.GKs * s[S_Xs]) * s[S_Xs]) * (V - Eks);
         float m = s[S_M];
         float INa = (((((c.GNa * m) * m) * m) * s[S_H]) * s[S_J]) * (V - Ena);
-        float INaK = (c.pmf_INaK * (Nai / (Nai + c.KmNa))) * a2_iNaK.y;
+        float INaK = (c.pmf_INaK * qdiv(Nai, Nai + c.KmNa)) * a2_iNaK.y;
         float IbCa = c.GbCa * (V - Eca);
         float IbNa = c.GbNa * (V - Ena);
         float IpK = (c.GpK * lut_col<TV_NCOL>(T.V, pv, TV_rec_ipK)) * VmEk;
@@ -309,27 +307,27 @@ struct TTP {
         float Iion = ((((((((((IKr + IKs) + IK1) + Ito) + INa) + IbNa) + ICaL) + IbCa) + INaK) + INaCa) + IpCa) + IpK;
 
         float Ileak = c.Vleak * (CaSR - Cai);
-        float Iup = sdiv(c.Vmaxup, 1.0f + sdiv(c.KupKup, Cai * Cai));
+        float Iup = qsdiv(c.Vmaxup, 1.0f + qsdiv(c.KupKup, Cai * Cai));
         float Ixfer = c.Vxfer * (CaSS - Cai);
         float diff_Ki = (-((((IK1 + Ito) + IKr) + IKs) - (2.0f * INaK) + IpK)) * c.invVcF_Cm;
         float diff_Nai = (-(((INa + IbNa) + (3.0f * INaK)) + (3.0f * INaCa))) * c.invVcF_Cm;
-        float ec = sdiv(c.EC, CaSR);
-        float kCaSR = c.maxsr - sdiv(c.dsr, 1.0f + (ec * ec));
+        float ec = qsdiv(c.EC, CaSR);
+        float kCaSR = c.maxsr - qsdiv(c.dsr, 1.0f + (ec * ec));
         float bc = Cai + c.Kbufc;
-        float diff_Cai = ((Ixfer - ((((IbCa + IpCa) - (2.0f * INaCa)) * c.inverseVcF2) * c.CAP)) -
-                          ((Iup - Ileak) * c.Vsr_Vc)) /
-                         (1.0f + (sdiv(c.BufcKbufc, bc) / bc));
+        float diff_Cai = qdiv((Ixfer - ((((IbCa + IpCa) - (2.0f * INaCa)) * c.inverseVcF2) * c.CAP)) -
+                                  ((Iup - Ileak) * c.Vsr_Vc),
+                              1.0f + qdiv(qsdiv(c.BufcKbufc, bc), bc));
         float R_ = s[S_R_];
         float diff_R_ = (c.k4 * (1.0f - R_)) - (((c.k2_ * kCaSR) * CaSS) * R_);
-        float k1 = sdiv(c.k1_, kCaSR);
+        float k1 = qsdiv(c.k1_, kCaSR);
         float cass2 = lut_col<3>(T.CaSS, pc, 0);
-        float O = ((k1 * cass2) * R_) / ((k1 * cass2) + c.k3);
+        float O = qdiv((k1 * cass2) * R_, (k1 * cass2) + c.k3);
         float Irel = (c.Vrel * O) * (CaSR - CaSS);
         float bsr = CaSR + c.Kbufsr;
-        float diff_CaSR = ((Iup - Irel) - Ileak) / (1.0f + (sdiv(c.BufsrKbufsr, bsr) / bsr));
+        float diff_CaSR = qdiv((Iup - Irel) - Ileak, 1.0f + qdiv(qsdiv(c.BufsrKbufsr, bsr), bsr));
         float bss = CaSS + c.Kbufss;
-        float diff_CaSS = ((((-Ixfer) * c.Vc_Vss) + (Irel * c.Vsr_Vss)) + (((-ICaL) * c.inverseVssF2) * c.CAP)) /
-                          (1.0f + (sdiv(c.BufssKbufss, bss) / bss));
+        float diff_CaSS = qdiv((((-Ixfer) * c.Vc_Vss) + (Irel * c.Vsr_Vss)) + (((-ICaL) * c.inverseVssF2) * c.CAP),
+                               1.0f + qdiv(qsdiv(c.BufssKbufss, bss), bss));
         s[S_CaSR] = CaSR + diff_CaSR * c.dt;
         s[S_CaSS] = CaSS + diff_CaSS * c.dt;
         s[S_Cai] = Cai + diff_Cai * c.dt;

@@ -2,9 +2,13 @@
 #pragma once
 #include <stdint.h>
 
+#include "cg_common.cuh"
 #include "tcb200.h"
 
 namespace tcb {
+
+// limits of the bounded device waits for this process (TCB_TEST_WAIT_STALL, see cg_common.cuh)
+cgk::WaitLimit wait_limit();
 
 struct MonoDev {
     int64_t n, n_pad, n_slices, nt;
@@ -26,7 +30,9 @@ struct MonoDev {
     int32_t max_iter, linear_guess, at_rt, per_frame;
     int32_t a_split;   // A == fp32(fp32(M*Cm) + K') verified at assembly
     float cm, dt;
-    int32_t snap_ring, pad;   // snapshot rows: 0 = one per frame, > 0 = ring of that many
+    int32_t snap_ring;        // snapshot rows: 0 = one per frame, > 0 = ring of that many
+    int32_t cg_per_sm;        // resident CG blocks per SM: 0 = most that fit, 1 or 2 pinned
+    cgk::WaitLimit wait;      // bounded-wait limits of the grid barriers
     float amp[TCB_MAX_STIMULI];
 };
 

@@ -21,14 +21,19 @@
 
 #include <mutex>
 
+#include "cg_common.cuh"
 #include "mono.cuh"
 #include "tcb_internal.h"
 
 namespace tcb {
+int validate_mono(const tcb_mono* m);
 namespace {
 
-constexpr int kNoAllocMaxBlocks = 2048;
+// Both CG kernels place their second partial buffer at scratch + 2 * cgk::kMaxBlocks
+// whatever the block count, so the array is sized from that constant.
+constexpr int kNoAllocMaxBlocks = cgk::kMaxBlocks;
 constexpr int kPartials = 4 * kNoAllocMaxBlocks;   // doubles: two parity buffers x 2 values x blocks
+static_assert(kPartials == 4 * cgk::kMaxBlocks, "static scratch must hold what tcb_mono_scratch_doubles() asks for");
 constexpr int kBarrierWords = 4;
 
 // Device scratch.  In host code `g_scratch` is only a stand-in symbol: its
@@ -73,12 +78,15 @@ extern "C" int tcb_mono_run_noalloc(const tcb_mono* m, int64_t step_begin, int64
     if (st) return st;
     local.scratch = static_cast<double*>(base);
     local.barrier = reinterpret_cast<uint32_t*>(static_cast<double*>(base) + kPartials);
+    // the struct is checked before anything touches the shared array
+    st = validate_mono(&local);
+    if (st) return st;
     if (step_begin < 1 || step_end > local.nt + 1 || step_begin > step_end)
         return fail(TCB_EINVAL, "tcb_mono_run_noalloc: step range outside [1, nt]");
     if (step_begin == step_end) return TCB_OK;
     MonoDev d = make_dev(&local);
     if (cg_blocks(d) > kNoAllocMaxBlocks)
-        return fail(TCB_ERANGE, "tcb_mono_run_noalloc: the CG launch needs more blocks than the static scratch holds (2048)");
+        return fail(TCB_ERANGE, "tcb_mono_run_noalloc: the CG launch needs more blocks than the static scratch holds");
     cudaStream_t s = as_stream(stream);
     TCB_CHECK_CUDA(cudaMemsetAsync(local.barrier, 0, kBarrierWords * sizeof(uint32_t), s));
     return tcb_mono_run(&local, step_begin, step_end, stream);

@@ -181,12 +181,17 @@ class Monodomain:
         elif snaps is not None:
             snaps[0] = u0
         t32, mask = self.stimuli.schedule(nt, self.dt)
+        # per-node arrays are n_pad long (the ionic kernels may read groups of nodes as
+        # one vector access); AT/RT are exposed as their first n entries
+        at_rt = torch.full((2, n_pad), -1.0, **f32)
+        bits = np.zeros(n_pad, dtype=np.uint32)
+        bits[:n] = self._stim_bits()
         sim = dict(
             x=x, bp=torch.zeros(n_pad, **f32), r=torch.zeros(n_pad, **f32), p=torch.zeros(n_pad, **f32),
             ap=torch.zeros(n_pad, **f32), z=torch.zeros(n_pad, **f32), p2=torch.zeros(n_pad, **f32),
-            at=torch.full((n,), -1.0, **f32), rt=torch.full((n,), -1.0, **f32),
+            at_rt=at_rt, at=at_rt[0, :n], rt=at_rt[1, :n],
             snaps=snaps, u0=u0, ring=ring, host_snaps=host_snaps,
-            stim_bits=torch.from_numpy(self._stim_bits().view(np.int32)).to(dev),
+            stim_bits=torch.from_numpy(bits.view(np.int32)).to(dev),
             step_t=torch.from_numpy(t32).to(dev), step_stim=torch.from_numpy(mask.view(np.int32)).to(dev),
             step_iters=torch.zeros(nt + 1, device=dev, dtype=torch.int32),
             counter=torch.tensor([1, 0, 0, 0], device=dev, dtype=torch.int32),
@@ -463,15 +468,25 @@ class Monodomain:
         return self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval,
                            snapshot_interval < self.T)
 
+    def autotune(self, steps=5, force=False):
+        """Choose the launch shapes of the prepared simulation's kernels (ionic
+        kernel instance, CG blocks per SM): the cached choice for this device and
+        problem shape, else each candidate timed on a scratch copy of the
+        simulation (``torchcor_b200.tune.tune_single``).  Returns the choice."""
+        from torchcor_b200 import tune
+        self.tuned = tune.tune_single(self, steps=steps, force=force)
+        return self.tuned
+
     def solve(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1,
-              verbose=True, result_path=None, snapshot_ring=None, graph_steps=100):
+              verbose=True, result_path=None, snapshot_ring=None, graph_steps=100, autotune=True):
         """monodomain.py:141-226.  ``snapshot_ring=R`` keeps only R snapshot frames on
         the device and streams every frame, as soon as it is written, into a pinned host
         tensor on a separate stream (``solutions`` is then that host tensor); the
         default keeps every frame on the device, as the reference does.
         ``graph_steps=G`` runs every whole G-step stretch of the loop as the replay of
         one CUDA graph of the same kernels (recorded once per solve); the results are
-        bit-identical to plain launches (``graph_steps=0``)."""
+        bit-identical to plain launches (``graph_steps=0``).  ``autotune`` picks the
+        kernels' launch shapes first (``autotune()``; cached per device and shape)."""
         self.result_path = Path(result_path) if result_path is not None else None
         if self.result_path is not None:
             self.result_path.mkdir(parents=True, exist_ok=True)
@@ -481,6 +496,8 @@ class Monodomain:
             raise ValueError("snapshot_ring must be a positive number of frames")
         sim = self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep,
                           snapshot_ring or 0)
+        if autotune:
+            self.autotune()
         t0 = time.time()
         ring = sim["ring"]
         if ring:

@@ -1,7 +1,15 @@
 """Autotuning of launch choices, with the choices cached on disk.
 
-The one runtime choice that depends on the hardware and on the shape of the
-work is the batched CG kernel variant: 2 = streaming, sized for 2 blocks per SM
+Single simulations (``tune_single``): the instance of the fused ionic kernel
+(1, 2 or 4 consecutive nodes per thread, each compiled for a register budget
+of some blocks per SM; ``_lib.ionic_variants``) and the blocks per SM of the
+CG kernel that keeps rows in shared memory (1 or 2, where the rows fit).  Each
+candidate is timed with CUDA events on a scratch copy of the simulation's
+mutable device buffers, from the simulation's current step, so the simulation
+itself is untouched; the key is the device, the model and log2 buckets of the
+node count and of the non-zeros per row.
+
+Batches (``tune_batch``): the batched CG kernel variant: 2 = streaming, sized for 2 blocks per SM
 (64 registers a thread, twice the warps to hide memory latency); 1 = streaming,
 1 block per SM (128 registers, no spills); 3 = 1 block per SM with the sliced-ELL
 streams staged in shared memory by bulk asynchronous copies (only where every
@@ -115,3 +123,100 @@ def tune_batch(batch, steps=10, cache=None, force=False):
     batch.set_cg(best)
     cache.put(key, {"cg_variant": best, "ms_per_step": {str(k): v for k, v in times.items()}})
     return best, times
+
+
+# ---------------------------------------------------------------- single simulations
+def single_key(device, n_nodes, nnz, model_name) -> str:
+    return (f"mono|{device_key(device)}|nodes2^{int(math.log2(max(n_nodes, 1)))}/"
+            f"nnz_per_row2^{int(math.log2(max(nnz / max(n_nodes, 1), 1.0)))}/{model_name}")
+
+
+class ScratchSim:
+    """Copies of a prepared simulation's mutable device buffers and a tcb_mono
+    pointing at them (snapshots off): trial launches leave the simulation as it was."""
+
+    def __init__(self, sim):
+        import ctypes as C
+        from torchcor_b200 import _lib
+        d = sim._sim
+        src = d["struct"]
+        self.orig = {"state": sim.ionic_model.state, "x": d["x"], "bp": d["bp"], "r": d["r"], "p": d["p"],
+                     "ap": d["ap"], "z": d["z"], "p2": d["p2"], "at_rt": d["at_rt"], "step_iters": d["step_iters"],
+                     "counter": d["counter"], "scratch": d["scratch"], "barrier": d["barrier"]}
+        self.buf = {k: v.clone() for k, v in self.orig.items()}
+        m = _lib.tcb_mono()
+        C.memmove(C.byref(m), C.byref(src), C.sizeof(m))
+        b = self.buf
+        m.state, m.x, m.bprime, m.r, m.p, m.ap, m.z, m.p2 = (_lib.ptr(b[k]) for k in
+                                                            ("state", "x", "bp", "r", "p", "ap", "z", "p2"))
+        m.at, m.rt = _lib.ptr(b["at_rt"][0]), _lib.ptr(b["at_rt"][1])
+        m.snapshots, m.snap_ring = None, 0
+        m.step_iters, m.counter = _lib.ptr(b["step_iters"]), _lib.ptr(b["counter"])
+        m.scratch, m.barrier = _lib.ptr(b["scratch"]), _lib.ptr(b["barrier"])
+        self.struct = m
+
+    def reset(self):
+        for k, v in self.orig.items():
+            self.buf[k].copy_(v)
+
+
+def time_steps(scratch, first, steps, stream):
+    """(ionic ms, CG ms) per step over ``steps`` steps from ``first`` on the scratch copy,
+    after one untimed step (the first launch of an instance loads it)."""
+    import ctypes as C
+    from torchcor_b200 import _lib
+    lib = _lib.load()
+    scratch.reset()
+    m = scratch.struct
+    _lib.check(lib.tcb_mono_run(C.byref(m), first, first + 1, stream.cuda_stream))
+    mi, mc = C.c_double(0.0), C.c_double(0.0)
+    _lib.check(lib.tcb_mono_profile(C.byref(m), first + 1, first + 1 + steps, stream.cuda_stream, C.byref(mi),
+                                    C.byref(mc)))
+    _lib.check(lib.tcb_mono_check(C.byref(m), stream.cuda_stream))
+    return mi.value / steps, mc.value / steps
+
+
+def tune_single(sim, steps=5, cache=None, force=False):
+    """Choose the ionic kernel instance and the CG blocks per SM for a prepared
+    ``Monodomain`` (after ``prepare`` or ``_setup``) and set them in its tcb_mono.
+
+    Uses the cached choice when there is one (unless ``force``); otherwise times
+    every candidate for ``steps`` steps on a scratch copy and records the fastest.
+    Needs ``steps + 1`` steps left; with fewer it keeps the defaults.  Returns the
+    choice ``{"ionic_variant": k, "cg_per_sm": c, ...}`` (with timings when measured)."""
+    import ctypes as C
+    from torchcor_b200 import _lib
+    cache = cache if cache is not None else TuneCache()
+    d = sim._sim
+    m = d["struct"]
+    model = sim.ionic_model
+    key = single_key(sim.device, int(m.n_nodes), int(sim.system.nnz), model.name)
+    hit = None if force else cache.get(key)
+    shapes = _lib.ionic_variants(model.model_id)
+    if hit is not None and 0 <= int(hit.get("ionic_variant", 0)) <= len(shapes):
+        m.ionic_variant, m.cg_per_sm = int(hit["ionic_variant"]), int(hit.get("cg_per_sm", 0))
+        return dict(hit, cached=True)
+    first = d["next_step"]
+    if sim.nt + 1 - first < steps + 1:
+        return {"ionic_variant": int(m.ionic_variant), "cg_per_sm": int(m.cg_per_sm), "measured": False}
+    stream = torch.cuda.current_stream(sim.device)
+    scratch = ScratchSim(sim)
+    t_ion = {}
+    for k in range(1, len(shapes) + 1):
+        scratch.struct.ionic_variant, scratch.struct.cg_per_sm = k, 0
+        t_ion[k] = time_steps(scratch, first, steps, stream)[0]
+    best_ion = min(t_ion, key=t_ion.get)
+    t_cg = {}
+    lib = _lib.load()
+    for c in (2, 1):
+        scratch.struct.ionic_variant, scratch.struct.cg_per_sm = best_ion, c
+        if lib.tcb_mono_cg_kernel(C.byref(scratch.struct)) != 1:   # rows do not fit: streaming kernel
+            continue
+        t_cg[c] = time_steps(scratch, first, steps, stream)[1]
+    best_cg = min(t_cg, key=t_cg.get) if t_cg else 0
+    del scratch
+    m.ionic_variant, m.cg_per_sm = best_ion, best_cg
+    choice = {"ionic_variant": best_ion, "cg_per_sm": best_cg, "ionic_shape": list(shapes[best_ion - 1]),
+              "ionic_ms": {str(k): v for k, v in t_ion.items()}, "cg_ms": {str(k): v for k, v in t_cg.items()}}
+    cache.put(key, choice)
+    return dict(choice, measured=True)
