@@ -1,4 +1,5 @@
 """Autotuner cache and keys (CPU); the timed choice on a GPU is in test_gpu_batch.py."""
+import ctypes as C
 import json
 
 from torchcor_b200 import tune
@@ -32,3 +33,16 @@ def test_batch_signature_buckets():
     b = tune.batch_signature([6000, 69000], ["ModifiedMS2v", "TenTusscherPanfilov"])
     assert a == b   # same log2 buckets and model set, order-free
     assert tune.batch_signature([5000] * 64, ["ModifiedMS2v"]) != tune.batch_signature([5000] * 2, ["ModifiedMS2v"])
+
+
+def test_ionic_variant_table(lib):
+    from torchcor_b200 import _lib
+    for model in (_lib.MODEL_MS, _lib.MODEL_TTP, _lib.MODEL_CRN):
+        shapes = _lib.ionic_variants(model)
+        assert len(shapes) >= 3
+        assert all(v in (1, 2, 4) and b >= 1 and f in (0, 1) for v, b, f in shapes)
+        assert any(v == 1 for v, _, _ in shapes)          # the fallback for unaligned arrays
+    cnt, v, b, f = (C.c_int32() for _ in range(4))
+    assert lib.tcb_ionic_variant(_lib.MODEL_TTP, 99, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f)) == \
+        _lib.TCB_ERANGE
+    assert lib.tcb_ionic_variant(7, 0, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f)) == _lib.TCB_EINVAL

@@ -69,7 +69,7 @@ __device__ __forceinline__ void ionic_tiles(const BatchWS* __restrict__ W, int g
         const int64_t node = (tile - first) * kBatchTile + threadIdx.x;
         if (step >= 1 && step <= sd.nt && node < sd.n) {
             const typename M::C& c = SHARED ? c0 : static_cast<const typename M::C*>(G.consts)[lo];
-            ionic_node<M>(sd, c, sT, sv, node);
+            ionic_node<M, QExact>(sd, c, sT, sv, node);
         }
     }
 }

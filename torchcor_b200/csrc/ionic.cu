@@ -5,13 +5,13 @@
 //
 // The fused kernel is instantiated for several launch shapes: 1, 2 or 4
 // consecutive nodes per thread (structure-of-arrays state read and written as
-// 4-, 8- or 16-byte vectors) and a register budget set by the blocks per SM it
-// is compiled for.  tcb_mono.ionic_variant picks one (the autotuner measures
-// them); every instance runs the same per-node arithmetic.
+// 4-, 8- or 16-byte vectors), a register budget set by the blocks per SM it is
+// compiled for, and a division/logarithm policy (QFast or QExact,
+// ionic_common.cuh).  tcb_mono.ionic_variant picks one (the autotuner measures
+// them); every instance runs the reference's per-node order of operations.
 //
-// Compiled with multiply-add contraction; the per-step division and logarithm
-// are the hardware forms (ionic_common.cuh).  Lookup tables are built in
-// tables.cu with separate roundings.
+// Compiled with multiply-add contraction.  Lookup tables are built in tables.cu
+// with separate roundings.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -41,19 +41,19 @@ __global__ void differentiate_kernel(typename M::C c, typename M::Tables T, floa
         float s[M::kStates];
 #pragma unroll
         for (int k = 0; k < M::kStates; ++k) s[k] = state[k * n_pad + i];
-        float d = M::step(v[i], s, c, T);
+        float d = M::template step<QFast>(v[i], s, c, T);
 #pragma unroll
         for (int k = 0; k < M::kStates; ++k) state[k * n_pad + i] = s[k];
         dv[i] = d;
     }
 }
 
-template <class M, int V, int MINB>
+template <class M, int V, int MINB, class Q>
 __global__ void __launch_bounds__(kThreads, MINB) mono_ionic_kernel(MonoDev d, typename M::C c, typename M::Tables T) {
     const StepView sv = step_view(d, d.counter[0]);
     const int64_t groups = (d.n + V - 1) / V;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (int64_t)gridDim.x * blockDim.x)
-        ionic_group<M, V>(d, c, T, sv, g * V);
+        ionic_group<M, V, Q>(d, c, T, sv, g * V);
 }
 
 __global__ void mono_finish_kernel(MonoDev d) {
@@ -74,40 +74,46 @@ __global__ void mono_finish_kernel(MonoDev d) {
 template <class M>
 using LaunchFn = int (*)(const MonoDev&, const typename M::C&, const typename M::Tables&, cudaStream_t);
 
-template <class M, int V, int MINB>
+template <class M, int V, int MINB, class Q>
 int launch_shape(const MonoDev& d, const typename M::C& c, const typename M::Tables& T, cudaStream_t s) {
-    mono_ionic_kernel<M, V, MINB><<<grid_for(ceil_div(d.n, V)), kThreads, 0, s>>>(d, c, T);
+    mono_ionic_kernel<M, V, MINB, Q><<<grid_for(ceil_div(d.n, V)), kThreads, 0, s>>>(d, c, T);
     TCB_CHECK_LAUNCH("mono ionic kernel");
     return TCB_OK;
 }
 
-// The instances of each model (nodes per thread, 256-thread blocks per SM the
-// register budget is set for); entry 0 is the default.
+// The instances of each model: nodes per thread, 256-thread blocks per SM the
+// register budget is set for, division/log policy (1 = QFast, 0 = QExact);
+// entry 0 is the default (the fastest measured on the million-node cubes).
 struct Shape {
-    int32_t nodes_per_thread, blocks_per_sm;
+    int32_t nodes_per_thread, blocks_per_sm, fast;
 };
 template <class M>
 struct Shapes;
 template <>
 struct Shapes<MS> {
-    static constexpr int kCount = 3;
-    static constexpr Shape shape[kCount] = {{1, 1}, {2, 1}, {4, 1}};
-    static constexpr LaunchFn<MS> fn[kCount] = {launch_shape<MS, 1, 1>, launch_shape<MS, 2, 1>, launch_shape<MS, 4, 1>};
+    static constexpr int kCount = 5;
+    static constexpr Shape shape[kCount] = {{4, 1, 0}, {1, 1, 0}, {2, 1, 0}, {4, 4, 0}, {4, 8, 0}};
+    static constexpr LaunchFn<MS> fn[kCount] = {launch_shape<MS, 4, 1, QExact>, launch_shape<MS, 1, 1, QExact>,
+                                                launch_shape<MS, 2, 1, QExact>, launch_shape<MS, 4, 4, QExact>,
+                                                launch_shape<MS, 4, 8, QExact>};
 };
 template <>
 struct Shapes<TTP> {
-    static constexpr int kCount = 6;
-    static constexpr Shape shape[kCount] = {{1, 6}, {1, 4}, {2, 4}, {2, 3}, {4, 3}, {4, 2}};
-    static constexpr LaunchFn<TTP> fn[kCount] = {launch_shape<TTP, 1, 6>, launch_shape<TTP, 1, 4>,
-                                                 launch_shape<TTP, 2, 4>, launch_shape<TTP, 2, 3>,
-                                                 launch_shape<TTP, 4, 3>, launch_shape<TTP, 4, 2>};
+    static constexpr int kCount = 8;
+    static constexpr Shape shape[kCount] = {{1, 4, 0}, {1, 6, 0}, {2, 3, 0}, {4, 2, 0},
+                                            {1, 2, 1}, {1, 3, 1}, {2, 2, 1}, {4, 1, 1}};
+    static constexpr LaunchFn<TTP> fn[kCount] = {
+        launch_shape<TTP, 1, 4, QExact>, launch_shape<TTP, 1, 6, QExact>, launch_shape<TTP, 2, 3, QExact>,
+        launch_shape<TTP, 4, 2, QExact>, launch_shape<TTP, 1, 2, QFast>,  launch_shape<TTP, 1, 3, QFast>,
+        launch_shape<TTP, 2, 2, QFast>,  launch_shape<TTP, 4, 1, QFast>};
 };
 template <>
 struct Shapes<CRN> {
-    static constexpr int kCount = 4;
-    static constexpr Shape shape[kCount] = {{1, 3}, {1, 2}, {2, 2}, {4, 1}};
-    static constexpr LaunchFn<CRN> fn[kCount] = {launch_shape<CRN, 1, 3>, launch_shape<CRN, 1, 2>,
-                                                 launch_shape<CRN, 2, 2>, launch_shape<CRN, 4, 1>};
+    static constexpr int kCount = 6;
+    static constexpr Shape shape[kCount] = {{2, 2, 1}, {1, 3, 1}, {1, 2, 1}, {4, 1, 1}, {1, 3, 0}, {2, 2, 0}};
+    static constexpr LaunchFn<CRN> fn[kCount] = {
+        launch_shape<CRN, 2, 2, QFast>, launch_shape<CRN, 1, 3, QFast>,  launch_shape<CRN, 1, 2, QFast>,
+        launch_shape<CRN, 4, 1, QFast>, launch_shape<CRN, 1, 3, QExact>, launch_shape<CRN, 2, 2, QExact>};
 };
 
 inline bool aligned(const void* p, unsigned bytes) { return ((uintptr_t)p & (bytes - 1)) == 0; }
@@ -150,12 +156,14 @@ int launch_mono_ionic(const tcb_mono* m, const MonoDev& d, cudaStream_t s) {
 }
 
 template <class M>
-int variant_info(int32_t variant, int32_t* count, int32_t* nodes_per_thread, int32_t* blocks_per_sm) {
+int variant_info(int32_t variant, int32_t* count, int32_t* nodes_per_thread, int32_t* blocks_per_sm,
+                 int32_t* fast) {
     *count = Shapes<M>::kCount;
     if (variant < 0 || variant > Shapes<M>::kCount) return fail(TCB_ERANGE, "no such ionic kernel variant");
     const Shape& sh = Shapes<M>::shape[variant > 0 ? variant - 1 : 0];
     *nodes_per_thread = sh.nodes_per_thread;
     *blocks_per_sm = sh.blocks_per_sm;
+    *fast = sh.fast;
     return TCB_OK;
 }
 
@@ -185,12 +193,13 @@ extern "C" int tcb_model_differentiate(int32_t model, const double* params, cons
 }
 
 extern "C" int tcb_ionic_variant(int32_t model, int32_t variant, int32_t* count, int32_t* nodes_per_thread,
-                                 int32_t* blocks_per_sm) {
-    if (!count || !nodes_per_thread || !blocks_per_sm) return fail(TCB_EINVAL, "tcb_ionic_variant: null output");
+                                 int32_t* blocks_per_sm, int32_t* fast_math) {
+    if (!count || !nodes_per_thread || !blocks_per_sm || !fast_math)
+        return fail(TCB_EINVAL, "tcb_ionic_variant: null output");
     switch (model) {
-        case TCB_MODEL_MS: return variant_info<MS>(variant, count, nodes_per_thread, blocks_per_sm);
-        case TCB_MODEL_TTP: return variant_info<TTP>(variant, count, nodes_per_thread, blocks_per_sm);
-        case TCB_MODEL_CRN: return variant_info<CRN>(variant, count, nodes_per_thread, blocks_per_sm);
+        case TCB_MODEL_MS: return variant_info<MS>(variant, count, nodes_per_thread, blocks_per_sm, fast_math);
+        case TCB_MODEL_TTP: return variant_info<TTP>(variant, count, nodes_per_thread, blocks_per_sm, fast_math);
+        case TCB_MODEL_CRN: return variant_info<CRN>(variant, count, nodes_per_thread, blocks_per_sm, fast_math);
     }
     return fail(TCB_EINVAL, "unknown ionic model");
 }

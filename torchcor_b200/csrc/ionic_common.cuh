@@ -10,9 +10,9 @@
 // Their grids pass through removable singularities where the last ulp decides
 // between a finite value and NaN, so they keep IEEE division.
 // The per-step updates (every node, every step) keep the reference's order of
-// operations but let the compiler fuse multiply-adds and use the hardware
-// division and logarithm (qdiv, qsdiv, qlog): a few ulp per operation, far
-// inside the 1e-3 membrane-potential tolerance, for fewer instructions.
+// operations but let the compiler fuse multiply-adds, and take their division
+// and logarithm from a policy (QFast or QExact below): a few ulp per operation,
+// far inside the 1e-3 membrane-potential tolerance.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -33,27 +33,39 @@ constexpr int count_names(const char* s) {
 // python_float / tensor
 TCB_HD float sdiv(float s, float t) { return (1.0f / t) * s; }
 
-// a / b in a per-step update: __fdividef (a times the hardware reciprocal of b,
-// within 2 ulp for |b| below 2^126; every denominator here is far smaller)
-TCB_HD float qdiv(float a, float b) {
+// Division and logarithm of the per-step updates, as a compile-time policy of
+// each kernel instance:
+//  * QFast: __fdividef (a times the hardware reciprocal of b, within 2 ulp for
+//    |b| below 2^126; every denominator here is far smaller) and __logf
+//    (absolute error below 2^-21.4 on [0.5, 2], a few ulp elsewhere; the
+//    arguments are positive concentration ratios).  Fewest instructions, but the
+//    compiler then schedules the table gathers far ahead, so it pays only with a
+//    large register budget.
+//  * QExact: IEEE division and logf, python_float / tensor as reciprocal times
+//    the float (PyTorch's order).  Under a tight register budget it spills far
+//    less.
+struct QFast {
+    static TCB_HD float div(float a, float b) {
 #ifdef __CUDA_ARCH__
-    return __fdividef(a, b);
+        return __fdividef(a, b);
 #else
-    return a / b;
+        return a / b;
 #endif
-}
-// python_float / tensor in a per-step update (reciprocal then product, as sdiv)
-TCB_HD float qsdiv(float s, float t) { return qdiv(s, t); }
-// natural logarithm in a per-step update (__logf: absolute error below 2^-21.4
-// on [0.5, 2], a few ulp elsewhere; the arguments here are positive
-// concentration ratios)
-TCB_HD float qlog(float x) {
+    }
+    static TCB_HD float sdiv(float s, float t) { return div(s, t); }
+    static TCB_HD float log(float x) {
 #ifdef __CUDA_ARCH__
-    return __logf(x);
+        return __logf(x);
 #else
-    return logf(x);
+        return logf(x);
 #endif
-}
+    }
+};
+struct QExact {
+    static TCB_HD float div(float a, float b) { return a / b; }
+    static TCB_HD float sdiv(float s, float t) { return (1.0f / t) * s; }
+    static TCB_HD float log(float x) { return logf(x); }
+};
 
 // torch.clamp(X, mn, mx) with NaN propagation
 TCB_HD float tclamp(float x, float mn, float mx) {
@@ -74,6 +86,7 @@ struct LutPos {
     float w, w1;  // w, 1 - w
 };
 
+template <class Q>
 TCB_HD LutPos lut_pos(float X, const Lut& L) {
     X = tclamp(X, L.mn, L.mx);
     float f = (X - L.mn) * L.step;   // X is clamped, so 0 <= f <= rows: 32-bit is enough
@@ -81,7 +94,7 @@ TCB_HD LutPos lut_pos(float X, const Lut& L) {
     idx = idx < 0 ? 0 : idx;
     idx = idx > L.mx_idx - 1 ? L.mx_idx - 1 : idx;
     float lo_pos = (float)idx * L.res + L.mn;
-    float w = qdiv(X - lo_pos, L.res);
+    float w = Q::div(X - lo_pos, L.res);
     LutPos p;
     p.lo = (int32_t)idx;
     p.w = w;

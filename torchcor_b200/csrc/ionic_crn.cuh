@@ -265,25 +265,26 @@ struct CRN {
     }
 
     // ------------------------------------------------ differentiate (:358-444)
-    // The reference's order of operations with the per-step division and
-    // logarithm (qdiv, qsdiv, qlog; ionic_common.cuh).
+    // The reference's order of operations; division and logarithm from the
+    // policy Q (QFast or QExact, ionic_common.cuh).
+    template <class Q>
     __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
-        LutPos pv = lut_pos(V, T.V);
-        LutPos pc = lut_pos(s[R_Cai], T.Cai);
+        LutPos pv = lut_pos<Q>(V, T.V);
+        LutPos pc = lut_pos<Q>(s[R_Cai], T.Cai);
 #define VR(col) lut_col<CV_NCOL>(T.V, pv, col)
 #define CR(col) lut_col<CC_NCOL>(T.Cai, pc, col)
-        float E_K = c.RTF * qlog(qsdiv(c.Ko, s[R_Ki]));
+        float E_K = c.RTF * Q::log(Q::sdiv(c.Ko, s[R_Ki]));
         float VmK = V - E_K;
         float ICaL = ((VR(CV_vrow_29) * s[R_d]) * s[R_f]) * s[R_f_Ca];
-        float IKACh = (c.ACh_term * (qsdiv(0.4516f, 1.0f + expf(qdiv(V + 59.53f, 17.18f))) + 0.0517f)) * VmK;
+        float IKACh = (c.ACh_term * (Q::sdiv(0.4516f, 1.0f + expf(Q::div(V + 59.53f, 17.18f))) + 0.0517f)) * VmK;
         float m = s[R_m];
         float INa = ((((VR(CV_vrow_7) * m) * m) * m) * s[R_h]) * s[R_j];
         float INaCa = VR(CV_vrow_31) - (s[R_Cai] * VR(CV_vrow_32));
         float vrow_13 = c.Gto * VmK;
         float vrow_18 = (c.factorGKur * VR(CV_GKur)) * VmK;
-        float vrow_21 = qdiv(c.GKr * VmK, 1.0f + expf(qdiv(V + 15.0f, 22.4f)));
+        float vrow_21 = Q::div(c.GKr * VmK, 1.0f + expf(Q::div(V + 15.0f, 22.4f)));
         float vrow_24 = c.GKs * VmK;
-        float IK1 = qdiv(c.GK1 * VmK, 1.0f + expf(0.07f * (V + 80.0f)));
+        float IK1 = Q::div(c.GK1 * VmK, 1.0f + expf(0.07f * (V + 80.0f)));
         float IKr = vrow_21 * s[R_xr];
         float IKs = (vrow_24 * s[R_xs]) * s[R_xs];
         float ua = s[R_ua], oa = s[R_oa];
@@ -294,14 +295,14 @@ struct CRN {
         float Iion = INa + IK1 + Ito + IKur + IKr + IKs + ICaL + IpCa + INaCa + VR(CV_IbNa) + INaK + IKACh;
 
         float Ca_rel = s[R_Ca_rel], Ca_up = s[R_Ca_up], u = s[R_u];
-        float Itr = qdiv(c.factorGtr * (Ca_up - Ca_rel), c.tau_tr);
+        float Itr = Q::div(c.factorGtr * (Ca_up - Ca_rel), c.tau_tr);
         float Irel = (((((c.factorGrel * u) * u) * s[R_v]) * c.k_rel) * s[R_w]) * (Ca_rel - CR(CC_conCa));
         float dIups = CR(CC_carow_1) - (c.maxIup_maxCaup * Ca_up);
         float cs = Ca_rel + c.KmCsqn;
-        float diff_Ca_rel = qdiv(Itr - Irel, 1.0f + qdiv(qsdiv(c.C_dCa_rel, cs), cs));
-        float diff_Ki = qdiv(-((((((Ito + IKr) + IKur) + IKs) + IK1) + IKACh) - (2.0f * INaK)), c.FVoli);
+        float diff_Ca_rel = Q::div(Itr - Irel, 1.0f + Q::div(Q::sdiv(c.C_dCa_rel, cs), cs));
+        float diff_Ki = Q::div(-((((((Ito + IKr) + IKur) + IKs) + IK1) + IKACh) - (2.0f * INaK)), c.FVoli);
         float diff_Ca_up = dIups - (Itr * c.C_dCaup);
-        float diff_Cai = qdiv(((c.C_B1d * (((INaCa + INaCa) - IpCa) - ICaL)) - (c.C_B1e * dIups)) + Irel, CR(CC_carow_2));
+        float diff_Cai = Q::div(((c.C_B1d * (((INaCa + INaCa) - IpCa) - ICaL)) - (c.C_B1e * dIups)) + Irel, CR(CC_carow_2));
         s[R_Ca_rel] = Ca_rel + diff_Ca_rel * c.dt;
         s[R_Ca_up] = Ca_up + diff_Ca_up * c.dt;
         float fCaA = CR(CC_f_Ca_A);
@@ -309,7 +310,7 @@ struct CRN {
         s[R_Ki] = s[R_Ki] + diff_Ki * c.dt;
 
         float fn = (c.C_Fn1 * Irel) - (c.C_Fn2 * (ICaL - (0.4f * INaCa)));
-        LutPos pf = lut_pos(fn, T.Fn);
+        LutPos pf = lut_pos<Q>(fn, T.Fn);
         s[R_d] = VR(CV_d_A) + VR(CV_d_B) * s[R_d];
         s[R_f] = VR(CV_f_A) + VR(CV_f_B) * s[R_f];
         s[R_f_Ca] = fCaA + c.fCa_B * s[R_f_Ca];

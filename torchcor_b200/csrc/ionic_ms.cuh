@@ -47,6 +47,7 @@ struct MS {
     }
 
     // ModifiedMS2v.differentiate (:36-44); returns dU and updates H
+    template <class Q>
     __host__ __device__ static float step(float U, float* s, const C& c, const Tables&) {
         float H = s[0];
         float Uad = (U - c.vmin) / c.DV;

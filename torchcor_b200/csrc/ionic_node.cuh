@@ -55,7 +55,7 @@ __device__ __forceinline__ float stim_sum(const MonoDev& d, uint32_t smask, uint
 
 // AT/RT and snapshot of the previous step, ionic update, stimulus and
 // b' = u*Cm + dt*du/100 + dt*Istim/100 (monodomain.py:117-128) for node i.
-template <class M>
+template <class M, class Q>
 __device__ __forceinline__ void ionic_node(const MonoDev& d, const typename M::C& c, const typename M::Tables& T,
                                            const StepView& sv, int64_t i) {
     const float v = sv.u[i];
@@ -64,15 +64,15 @@ __device__ __forceinline__ void ionic_node(const MonoDev& d, const typename M::C
     float s[M::kStates];
 #pragma unroll
     for (int k = 0; k < M::kStates; ++k) s[k] = d.state[k * d.n_pad + i];
-    const float dV = M::step(v, s, c, T);
+    const float dV = M::template step<Q>(v, s, c, T);
 #pragma unroll
     for (int k = 0; k < M::kStates; ++k) d.state[k * d.n_pad + i] = s[k];
     // b = u*Cm + dt*du, du = dV/100  (monodomain.py:117-118)
-    float b = v * d.cm + d.dt * qdiv(dV, 100.0f);
+    float b = v * d.cm + d.dt * Q::div(dV, 100.0f);
     if (sv.smask) {
         // Istim/100 (monodomain.py:127), b += dt*Istim (:128)
         const uint32_t bits = d.stim_bits[i] & sv.smask;
-        if (bits) b = b + d.dt * qdiv(stim_sum(d, sv.smask, bits), 100.0f);
+        if (bits) b = b + d.dt * Q::div(stim_sum(d, sv.smask, bits), 100.0f);
     }
     d.bp[i] = b;
 }
@@ -101,16 +101,17 @@ __device__ __forceinline__ void st_nodes(float* __restrict__ p, const float (&v)
     else *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
 }
 
-// ionic_node for the V consecutive nodes i0 .. i0+V-1 (V = 1, 2 or 4), with the
+// ionic_node for the V consecutive nodes i0 .. i0+V-1 (V = 1, 2 or 4; Q the
+// division policy), with the
 // per-node arrays moved as vectors for V > 1.  Nodes between n and n_pad are
 // padding: their ionic arithmetic runs on memory that exists but nothing reads
 // its results; their u stays 0, so AT/RT are never set for them, and snapshots
 // are written for real nodes only.
-template <class M, int V>
+template <class M, int V, class Q>
 __device__ __forceinline__ void ionic_group(const MonoDev& d, const typename M::C& c, const typename M::Tables& T,
                                             const StepView& sv, int64_t i0) {
     if constexpr (V == 1) {
-        ionic_node<M>(d, c, T, sv, i0);
+        ionic_node<M, Q>(d, c, T, sv, i0);
     } else {
         float v[V];
         ld_nodes<V>(sv.u + i0, v);
@@ -142,7 +143,7 @@ __device__ __forceinline__ void ionic_group(const MonoDev& d, const typename M::
         }
         float b[V];
 #pragma unroll
-        for (int j = 0; j < V; ++j) b[j] = v[j] * d.cm + d.dt * qdiv(M::step(v[j], s[j], c, T), 100.0f);
+        for (int j = 0; j < V; ++j) b[j] = v[j] * d.cm + d.dt * Q::div(M::template step<Q>(v[j], s[j], c, T), 100.0f);
 #pragma unroll
         for (int k = 0; k < M::kStates; ++k) {
             float t[V];
@@ -156,7 +157,7 @@ __device__ __forceinline__ void ionic_group(const MonoDev& d, const typename M::
 #pragma unroll
             for (int j = 0; j < V; ++j) {
                 const uint32_t on = bits[j] & sv.smask;
-                if (on) b[j] = b[j] + d.dt * qdiv(stim_sum(d, sv.smask, on), 100.0f);
+                if (on) b[j] = b[j] + d.dt * Q::div(stim_sum(d, sv.smask, on), 100.0f);
             }
         }
         st_nodes<V>(d.bp + i0, b);

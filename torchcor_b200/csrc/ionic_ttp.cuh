@@ -273,19 +273,20 @@ struct TTP {
     }
 
     // ---------------------------------------------------- differentiate (:353-454)
-    // The reference's order of operations with the per-step division and
-    // logarithm (qdiv, qsdiv, qlog; ionic_common.cuh).
+    // The reference's order of operations; division and logarithm from the
+    // policy Q (QFast or QExact, ionic_common.cuh).
+    template <class Q>
     __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
-        LutPos pv = lut_pos(V, T.V);
+        LutPos pv = lut_pos<Q>(V, T.V);
         const float CaSR = s[S_CaSR], CaSS = s[S_CaSS], Cai = s[S_Cai], Ki = s[S_Ki], Nai = s[S_Nai];
-        LutPos pc = lut_pos(CaSS, T.CaSS);
-        float Eca = c.halfRTONF * qlog(qsdiv(c.Cao, Cai));
-        float Ek = c.RTONF * qlog(qsdiv(c.Ko, Ki));
-        float Eks = c.RTONF * qlog(qsdiv(c.KoNa, Ki + (c.pKNa * Nai)));
-        float Ena = c.RTONF * qlog(qsdiv(c.Nao, Nai));
-        float IpCa = qdiv(c.GpCa * Cai, Cai + c.KpCa);
+        LutPos pc = lut_pos<Q>(CaSS, T.CaSS);
+        float Eca = c.halfRTONF * Q::log(Q::sdiv(c.Cao, Cai));
+        float Ek = c.RTONF * Q::log(Q::sdiv(c.Ko, Ki));
+        float Eks = c.RTONF * Q::log(Q::sdiv(c.KoNa, Ki + (c.pKNa * Nai)));
+        float Ena = c.RTONF * Q::log(Q::sdiv(c.Nao, Nai));
+        float IpCa = Q::div(c.GpCa * Cai, Cai + c.KpCa);
         float v15 = V - 15.0f;
-        float a1 = c.ga1 * ((V == 15.0f) ? c.halfFRT : qdiv(v15, expm1f((2.0f * v15) * c.F_RT)));
+        float a1 = c.ga1 * ((V == 15.0f) ? c.halfFRT : Q::div(v15, expm1f((2.0f * v15) * c.F_RT)));
         const float2 a2_iNaK = lut_pair<TV_NCOL>(T.V, pv, TV_a2);  // TV_a2, TV_rec_iNaK
         float ICaL_A = a1 * a2_iNaK.x;
         float ICaL_B = a1 * c.Cao;
@@ -294,12 +295,12 @@ struct TTP {
         float IKs = ((c.GKs * s[S_Xs]) * s[S_Xs]) * (V - Eks);
         float m = s[S_M];
         float INa = (((((c.GNa * m) * m) * m) * s[S_H]) * s[S_J]) * (V - Ena);
-        float INaK = (c.pmf_INaK * qdiv(Nai, Nai + c.KmNa)) * a2_iNaK.y;
+        float INaK = (c.pmf_INaK * Q::div(Nai, Nai + c.KmNa)) * a2_iNaK.y;
         float IbCa = c.GbCa * (V - Eca);
         float IbNa = c.GbNa * (V - Ena);
         float IpK = (c.GpK * lut_col<TV_NCOL>(T.V, pv, TV_rec_ipK)) * VmEk;
         float Ito = ((c.Gto * s[S_R]) * s[S_S]) * VmEk;
-        LutPos pe = lut_pos(VmEk, T.VEk);
+        LutPos pe = lut_pos<Q>(VmEk, T.VEk);
         float ICaL = (((s[S_D] * s[S_F]) * s[S_F2]) * s[S_FCaSS]) * ((ICaL_A * CaSS) - ICaL_B);
         const float2 naca = lut_pair<TV_NCOL>(T.V, pv, TV_INaCa_A);
         float INaCa = (((naca.x * Nai) * Nai) * Nai) - (naca.y * Cai);
@@ -307,27 +308,27 @@ struct TTP {
         float Iion = ((((((((((IKr + IKs) + IK1) + Ito) + INa) + IbNa) + ICaL) + IbCa) + INaK) + INaCa) + IpCa) + IpK;
 
         float Ileak = c.Vleak * (CaSR - Cai);
-        float Iup = qsdiv(c.Vmaxup, 1.0f + qsdiv(c.KupKup, Cai * Cai));
+        float Iup = Q::sdiv(c.Vmaxup, 1.0f + Q::sdiv(c.KupKup, Cai * Cai));
         float Ixfer = c.Vxfer * (CaSS - Cai);
         float diff_Ki = (-((((IK1 + Ito) + IKr) + IKs) - (2.0f * INaK) + IpK)) * c.invVcF_Cm;
         float diff_Nai = (-(((INa + IbNa) + (3.0f * INaK)) + (3.0f * INaCa))) * c.invVcF_Cm;
-        float ec = qsdiv(c.EC, CaSR);
-        float kCaSR = c.maxsr - qsdiv(c.dsr, 1.0f + (ec * ec));
+        float ec = Q::sdiv(c.EC, CaSR);
+        float kCaSR = c.maxsr - Q::sdiv(c.dsr, 1.0f + (ec * ec));
         float bc = Cai + c.Kbufc;
-        float diff_Cai = qdiv((Ixfer - ((((IbCa + IpCa) - (2.0f * INaCa)) * c.inverseVcF2) * c.CAP)) -
+        float diff_Cai = Q::div((Ixfer - ((((IbCa + IpCa) - (2.0f * INaCa)) * c.inverseVcF2) * c.CAP)) -
                                   ((Iup - Ileak) * c.Vsr_Vc),
-                              1.0f + qdiv(qsdiv(c.BufcKbufc, bc), bc));
+                              1.0f + Q::div(Q::sdiv(c.BufcKbufc, bc), bc));
         float R_ = s[S_R_];
         float diff_R_ = (c.k4 * (1.0f - R_)) - (((c.k2_ * kCaSR) * CaSS) * R_);
-        float k1 = qsdiv(c.k1_, kCaSR);
+        float k1 = Q::sdiv(c.k1_, kCaSR);
         float cass2 = lut_col<3>(T.CaSS, pc, 0);
-        float O = qdiv((k1 * cass2) * R_, (k1 * cass2) + c.k3);
+        float O = Q::div((k1 * cass2) * R_, (k1 * cass2) + c.k3);
         float Irel = (c.Vrel * O) * (CaSR - CaSS);
         float bsr = CaSR + c.Kbufsr;
-        float diff_CaSR = qdiv((Iup - Irel) - Ileak, 1.0f + qdiv(qsdiv(c.BufsrKbufsr, bsr), bsr));
+        float diff_CaSR = Q::div((Iup - Irel) - Ileak, 1.0f + Q::div(Q::sdiv(c.BufsrKbufsr, bsr), bsr));
         float bss = CaSS + c.Kbufss;
-        float diff_CaSS = qdiv((((-Ixfer) * c.Vc_Vss) + (Irel * c.Vsr_Vss)) + (((-ICaL) * c.inverseVssF2) * c.CAP),
-                               1.0f + qdiv(qsdiv(c.BufssKbufss, bss), bss));
+        float diff_CaSS = Q::div((((-Ixfer) * c.Vc_Vss) + (Irel * c.Vsr_Vss)) + (((-ICaL) * c.inverseVssF2) * c.CAP),
+                               1.0f + Q::div(Q::sdiv(c.BufssKbufss, bss), bss));
         s[S_CaSR] = CaSR + diff_CaSR * c.dt;
         s[S_CaSS] = CaSS + diff_CaSS * c.dt;
         s[S_Cai] = Cai + diff_Cai * c.dt;
