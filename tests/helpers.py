@@ -66,3 +66,17 @@ def case_mesh_dir(case, root):
     d = Path(root) / case["name"]
     C.write_case_mesh(case, d)
     return d
+
+
+def record_parity(case_name, reference, **metrics):
+    """Append one measured-error record (JSON line) to $TCB_PARITY_REPORT, if set."""
+    import json
+    import os
+    path = os.environ.get("TCB_PARITY_REPORT")
+    if not path:
+        return
+    rec = {"case": case_name, "reference": reference}
+    rec.update({k: (float(v) if isinstance(v, (np.floating, float)) else int(v) if isinstance(v, (np.integer, int))
+                    else v) for k, v in metrics.items()})
+    with open(path, "a") as f:
+        f.write(json.dumps(rec) + "\n")

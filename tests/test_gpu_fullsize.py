@@ -1,0 +1,116 @@
+"""Parity at the benchmark workloads' full size, against fixtures the reference
+itself produced (tests/golden/make_golden.py, compact format).
+
+* cfg2: ten Tusscher-Panfilov ENDO on the 100^3-cell tet cube (1,030,301 nodes,
+  6,000,000 tets, rotating fibres, two conductivity regions, corner stimuli at
+  t = 0 and 5 ms), the first 40 ms (4,000 steps, both stimuli, the whole cube
+  activates);
+* cfg3: Courtemanche on the level-7 icosphere (163,842 nodes, 327,680
+  triangles, random tangent fibres, cap stimulus), T = 400 ms (20,000 steps at
+  dt 0.02: activation and repolarisation).
+
+Each is compared with the reference's float32 run and with its float64 run:
+CSR pattern digest equal; matrix sums within 1e-5; activation/repolarisation
+step within one step at every node; max |dVm| <= 1e-3 * max |Vm_ref| on a
+32,768-node sample at the stored frames; total CG iterations within 2 %.  The
+measured errors go to $TCB_PARITY_REPORT when it is set.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from tests.golden import cases as C
+from tests.helpers import device_ionic, golden, record_parity
+
+pytestmark = pytest.mark.gpu
+
+
+def _digest(rowptr, col):
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(rowptr, dtype="<i4").tobytes())
+    h.update(np.ascontiguousarray(col, dtype="<i4").tobytes())
+    return h.hexdigest()
+
+
+def _steps(times, dt):
+    t = np.asarray(times, dtype=np.float64)
+    return np.where(t < 0, -1, np.rint(t / dt)).astype(np.int64)
+
+
+@pytest.fixture(scope="module")
+def runs(cuda):
+    """Device runs of the full-size cases (built once per module)."""
+    from torchcor_b200 import meshgen
+    from torchcor_b200.simulator import Monodomain
+    out = {}
+    for name in ("cfg2_ttp_f32", "cfg3_crn_f32"):
+        case = C.case(name)
+        nodes_um, elems, reg, fib = C.mesh_arrays(case)
+        stims = [C.stimulus_nodes(case, s["nodes"], nodes_um) for s in case["stimuli"]]
+        nodes_rt, fib_rt = meshgen.roundtrip(nodes_um, fib)        # what the reference read from text
+        sim = Monodomain(device_ionic(case, cuda), T=case["T"], dt=case["dt"], device=cuda)
+        sim.load_arrays(nodes_rt / 1000.0, elems, reg, fib_rt)
+        for c in case["conductivity"]:
+            sim.add_conductivity(**c)
+        for s, region in zip(case["stimuli"], stims):
+            sim.add_stimulus(None, s["start"], s["duration"], s["intensity"], region=region)
+        total = sim.solve(case["tol"], case["tol"], case["max_iter"], verbose=False, snapshot_interval=1)
+        sy = sim.system
+        out[name] = dict(
+            case=case, total=int(total), iters=sim._sim["step_iters"][1:sim.nt + 1].cpu().numpy(),
+            at=sim.activation_time.cpu().numpy(), rt=sim.repolarization_time.cpu().numpy(),
+            vm=sim.solutions.cpu().numpy(), digest=_digest(sy.rowptr.cpu().numpy(), sy.col.cpu().numpy()),
+            nnz=int(sy.nnz), m_sum=float(sy.m_val.double().sum()), k_abs=float(sy.k_val.double().abs().sum()),
+            a_sum=float(sy.a_val.double().sum()))
+        del sim
+    return out
+
+
+def _compare(run, ref_name):
+    case = run["case"]
+    g = golden(ref_name)
+    nt = int(case["T"] / case["dt"])
+    at, rt = _steps(run["at"], case["dt"]), _steps(run["rt"], case["dt"])
+    at_ref, rt_ref = g["AT_step"].astype(np.int64), g["RT_step"].astype(np.int64)
+    errs = {}
+    for nm, got, want in (("at", at, at_ref), ("rt", rt, rt_ref)):
+        both = (got >= 0) & (want >= 0)
+        errs[nm + "_max_steps"] = int(np.abs(got[both] - want[both]).max()) if both.any() else 0
+        # a time may be set in one run and not the other only at the last step
+        only = (got >= 0) != (want >= 0)
+        errs[nm + "_unmatched"] = int(only.sum())
+        errs[nm + "_unmatched_before_end"] = int((only & (np.maximum(got, want) < nt)).sum())
+        errs[nm + "_set"] = int((want >= 0).sum())
+    vm = run["vm"][g["Vm_idx"]][:, g["Vm_nodes"]]
+    errs["vm_rel"] = float(np.abs(vm.astype(np.float64) - g["Vm"]).max() / np.abs(g["Vm"]).max())
+    errs["vm_absmax_rel"] = float(np.abs(np.abs(run["vm"]).max(axis=1) - g["Vm_absmax"]).max() /
+                                  g["Vm_absmax"].max())
+    errs["iters_total"] = run["total"]
+    errs["iters_total_ref"] = int(g["n_total_iter"])
+    errs["iters_steps_equal_frac"] = float((run["iters"] == g["iters"]).mean())
+    record_parity(case["name"], ref_name, **errs)
+    assert errs["at_max_steps"] <= 1 and errs["at_unmatched_before_end"] == 0, errs
+    assert errs["rt_max_steps"] <= 1 and errs["rt_unmatched_before_end"] == 0, errs
+    assert errs["vm_rel"] <= 1e-3 and errs["vm_absmax_rel"] <= 1e-3, errs
+    ref_total = int(g["n_total_iter"])
+    assert abs(run["total"] - ref_total) <= max(3, ref_total // 50), errs
+    return g, errs
+
+
+@pytest.mark.parametrize("name", ["cfg2_ttp_f32", "cfg3_crn_f32"])
+def test_fullsize_matches_reference_float32(lib, runs, name):
+    run = runs[name]
+    g, errs = _compare(run, name)
+    assert run["digest"] == str(g["pattern_sha256"]) and run["nnz"] == int(g["nnz"])
+    for got, key in ((run["m_sum"], "M_sum"), (run["k_abs"], "K_abs_sum"), (run["a_sum"], "A_sum")):
+        assert abs(got - float(g[key])) <= 1e-5 * abs(float(g[key])), key
+    assert errs["at_set"] > 0.9 * len(run["at"])              # the fronts cross the whole mesh
+    if name.startswith("cfg3"):
+        assert errs["rt_set"] > 0.9 * len(run["rt"])          # and it repolarises
+
+
+@pytest.mark.parametrize("name,ref64", [("cfg2_ttp_f32", "cfg2_ttp_f64"), ("cfg3_crn_f32", "cfg3_crn_f64")])
+def test_fullsize_error_against_float64_reference(lib, runs, name, ref64):
+    """The float32 device path (float64 CG reductions) against the reference run in float64."""
+    _compare(runs[name], ref64)

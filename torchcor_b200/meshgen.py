@@ -178,9 +178,15 @@ def write_vtx(path, idx):
         np.savetxt(f, idx, fmt="%d")
 
 
+def _decimal_roundtrip(a, fmt):
+    """float(fmt % x) for every x of ``a``, formatting each distinct value once."""
+    a = np.asarray(a, dtype=np.float64)
+    u, inv = np.unique(a.ravel(), return_inverse=True)
+    r = np.array([float(fmt % x) for x in u], dtype=np.float64)
+    return r[inv].reshape(a.shape)
+
+
 def roundtrip(nodes_um, fibres):
     """The values ``load_mesh`` would read back from the files ``write_opencarp``
     writes (``%.6f`` nodes, ``%.8f`` fibres), for in-memory use."""
-    n = np.array([float("%.6f" % x) for x in nodes_um.ravel()]).reshape(nodes_um.shape)
-    f = np.array([float("%.8f" % x) for x in fibres.ravel()]).reshape(fibres.shape)
-    return n, f
+    return _decimal_roundtrip(nodes_um, "%.6f"), _decimal_roundtrip(fibres, "%.8f")
