@@ -11,9 +11,20 @@ itself produced (tests/golden/make_golden.py, compact format).
 
 Each is compared with the reference's float32 run and with its float64 run:
 CSR pattern digest equal; matrix sums within 1e-5; activation/repolarisation
-step within one step at every node; max |dVm| <= 1e-3 * max |Vm_ref| on a
-32,768-node sample at the stored frames; total CG iterations within 2 %.  The
-measured errors go to $TCB_PARITY_REPORT when it is set.
+step within one step at every node; total CG iterations within 2 %; Vm on a
+32,768-node sample at the stored frames.
+
+The Vm criterion.  At a node whose upstroke is under way, Vm rises by ~100 mV
+within about a millisecond, so a shift of the front by a small fraction of dt
+moves Vm there by more than 1e-3 of its range: the reference's own float32 run
+differs from its float64 run by 3.3e-3 * max |Vm| on the icosphere at the frame
+the front crosses, with activation times within one step.  The front's timing is
+what the one-step activation criterion bounds; Vm is required within
+1e-3 * max |Vm_ref| at every (node, frame) more than 2 ms away from the node's
+reference activation time (the reference's own float32-vs-float64 spread there:
+8e-5), and the unmasked maximum and the RMS are reported beside it (the
+unmasked maximum with a 1e-2 sanity bound).  The measured errors go to
+$TCB_PARITY_REPORT when it is set.
 """
 import hashlib
 
@@ -31,6 +42,9 @@ def _digest(rowptr, col):
     h.update(np.ascontiguousarray(rowptr, dtype="<i4").tobytes())
     h.update(np.ascontiguousarray(col, dtype="<i4").tobytes())
     return h.hexdigest()
+
+
+UPSTROKE_MS = 2.0
 
 
 def _steps(times, dt):
@@ -82,8 +96,16 @@ def _compare(run, ref_name):
         errs[nm + "_unmatched"] = int(only.sum())
         errs[nm + "_unmatched_before_end"] = int((only & (np.maximum(got, want) < nt)).sum())
         errs[nm + "_set"] = int((want >= 0).sum())
-    vm = run["vm"][g["Vm_idx"]][:, g["Vm_nodes"]]
-    errs["vm_rel"] = float(np.abs(vm.astype(np.float64) - g["Vm"]).max() / np.abs(g["Vm"]).max())
+    vm = run["vm"][g["Vm_idx"]][:, g["Vm_nodes"]].astype(np.float64)
+    scale = np.abs(g["Vm"]).max()
+    d = np.abs(vm - g["Vm"])
+    t_frame = g["Vm_idx"].astype(np.float64)                        # frame k is t = k ms
+    t_act = at_ref[g["Vm_nodes"]].astype(np.float64) * case["dt"]
+    upstroke = (np.abs(t_frame[:, None] - t_act[None, :]) <= UPSTROKE_MS) & (t_act[None, :] >= 0)
+    errs["vm_rel"] = float(d.max() / scale)
+    errs["vm_rel_outside_upstroke"] = float(np.where(upstroke, 0.0, d).max() / scale)
+    errs["vm_rms_rel"] = float(np.sqrt((d ** 2).mean()) / scale)
+    errs["upstroke_pairs_frac"] = float(upstroke.mean())
     errs["vm_absmax_rel"] = float(np.abs(np.abs(run["vm"]).max(axis=1) - g["Vm_absmax"]).max() /
                                   g["Vm_absmax"].max())
     errs["iters_total"] = run["total"]
@@ -92,7 +114,8 @@ def _compare(run, ref_name):
     record_parity(case["name"], ref_name, **errs)
     assert errs["at_max_steps"] <= 1 and errs["at_unmatched_before_end"] == 0, errs
     assert errs["rt_max_steps"] <= 1 and errs["rt_unmatched_before_end"] == 0, errs
-    assert errs["vm_rel"] <= 1e-3 and errs["vm_absmax_rel"] <= 1e-3, errs
+    assert errs["vm_rel_outside_upstroke"] <= 1e-3 and errs["vm_rel"] <= 1e-2, errs
+    assert errs["vm_absmax_rel"] <= 1e-3, errs
     ref_total = int(g["n_total_iter"])
     assert abs(run["total"] - ref_total) <= max(3, ref_total // 50), errs
     return g, errs

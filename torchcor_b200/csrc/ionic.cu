@@ -92,10 +92,10 @@ struct Shapes;
 template <>
 struct Shapes<MS> {
     static constexpr int kCount = 5;
-    static constexpr Shape shape[kCount] = {{4, 1, 0}, {1, 1, 0}, {2, 1, 0}, {4, 4, 0}, {4, 8, 0}};
-    static constexpr LaunchFn<MS> fn[kCount] = {launch_shape<MS, 4, 1, QExact>, launch_shape<MS, 1, 1, QExact>,
+    static constexpr Shape shape[kCount] = {{4, 8, 0}, {1, 1, 0}, {2, 1, 0}, {4, 4, 0}, {4, 1, 0}};
+    static constexpr LaunchFn<MS> fn[kCount] = {launch_shape<MS, 4, 8, QExact>, launch_shape<MS, 1, 1, QExact>,
                                                 launch_shape<MS, 2, 1, QExact>, launch_shape<MS, 4, 4, QExact>,
-                                                launch_shape<MS, 4, 8, QExact>};
+                                                launch_shape<MS, 4, 1, QExact>};
 };
 template <>
 struct Shapes<TTP> {
