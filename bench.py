@@ -3,18 +3,27 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tcb|reference]
 
-Workload (default ``ttp_cube``): ten Tusscher-Panfilov ENDO on a 100^3-cell
-tetrahedral cube (1,030,301 nodes, 6 M tets), see torchcor_b200/workloads.py.
-A step is one monodomain time step: ionic update + stimulus + LAT/RT,
-right-hand side, Jacobi-PCG to atol = rtol = 1e-5.
+Default run (one JSON line):
 
-``--impl tcb`` (default): K steps timed with CUDA events on the launch stream
-after W warm-up steps, barrier + synchronize on both sides, max over ranks;
-each rank runs an independent replica (the reference has no domain
-decomposition: "replicas only").  Prints one JSON line with value (node-steps/s,
-whole job), e2e (one full solve through the public API from host arrays),
-roofline (CG kernel, algorithmic bytes / event time vs measured HBM peak),
-clocks and the CPU baseline (the oracle on the same workload, host cores).
+* headline, ``ttp_cube``: ten Tusscher-Panfilov ENDO on a 100^3-cell tetrahedral
+  cube (1,030,301 nodes, 6 M tets), see torchcor_b200/workloads.py.  A step is
+  one monodomain time step: ionic update + stimulus + LAT/RT, right-hand side,
+  Jacobi-PCG to atol = rtol = 1e-5.  After W warm-up steps the run continues
+  untimed to step 400, a per-kernel profile window (steps 401..600, CUDA events
+  around every launch, for the roofline) follows, and the K timed steps start at
+  step 601 -- after the second stimulus (t = 5 ms), while the fronts travel and
+  CG iterates.  K steps timed with CUDA events on the launch stream (replays of
+  100-step CUDA graphs), barrier + synchronize on both sides, max over ranks;
+  each rank runs an independent replica ("replicas only").  Beside it: the same
+  workload's whole T = 100 ms run timed on the device (``full_run``), ``e2e`` (one
+  ``Monodomain.solve`` through the public API from host arrays), the roofline of
+  the dominant kernel, the CPU baseline, and clocks sampled over all of it.
+* ``batch``: 64 cubes of 16..64 nodes per edge, Mitchell-Schaeffer/TTP 50/50,
+  stepped together (``MonodomainBatch``) against the same simulations one after
+  the other on the single-simulation path, plus a full batched run from host
+  arrays (``batch.e2e``).
+* ``serving``: a Poisson stream of requests (``--requests``, default 128) served
+  with continuous batching: p50/p99 latency, throughput, GPU-busy fraction.
 
 ``--impl reference``: rank 0 times the oracle (CPU restatement of the
 reference path, torch CPU with every host thread) on the same workload:
@@ -52,50 +61,75 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms from the
+    first ``mark`` to ``stop``; ``summary`` covers the samples taken inside the
+    marked (GPU-busy) segments only.  ``mark(name)`` opens a segment,
+    ``mark(None)`` closes the current one."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.samples = []            # (host time, line)
+        self.segments = []           # [name, t_open, t_close or None]
+        self.thread = None
 
-    def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
-        return self
+    def _read(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                self.samples.append((time.perf_counter(), line))
 
-    def __exit__(self, *a):
-        self.lines = []
-        if self.proc is not None:
+    def mark(self, name):
+        now = time.perf_counter()
+        if self.segments and self.segments[-1][2] is None:
+            self.segments[-1][2] = now
+        if name is None:
+            return
+        if self.proc is None:
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.thread = threading.Thread(target=self._read, daemon=True)
+                self.thread.start()
+            except OSError:
+                self.proc = False
+        self.segments.append([name, now, None])
+
+    def stop(self):
+        self.mark(None)
+        if self.proc:
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.thread.join(timeout=5)
 
-    def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            f = [x.strip() for x in l.split(",")]
+    def summary(self, names=None):
+        sm, mx, reasons, per = [], None, set(), {}
+        for t, line in self.samples:
+            seg = next((g for g in self.segments if g[1] <= t <= (g[2] if g[2] is not None else float("inf"))),
+                       None)
+            if seg is None or (names is not None and seg[0] not in names):
+                continue
+            f = [x.strip() for x in line.split(",")]
             try:
-                sm.append(float(f[1]))
+                v = float(f[1])
                 mx = float(f[2])
             except (ValueError, IndexError):
                 continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
+            sm.append(v)
+            per.setdefault(seg[0], []).append(v)
+            for nm, r in zip(self.NAMES, f[5:9]):
+                if r.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "segments": {k: {"samples": len(v), "sm_mhz": float(np.median(v))}
+                                                 for k, v in per.items()}}
 
 
 def dist_setup(impl):
@@ -193,13 +227,18 @@ def reference_arm(a, wl, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def tcb_arm(a, wl, world, rank, local):
+# the timed window starts after the second stimulus of the headline workload (t = 5 ms)
+FIRST_TIMED_STEP = 601
+
+
+def tcb_arm(a, wl, world, rank, local, clk):
     from torchcor_b200 import _lib
     from torchcor_b200.workloads import algorithmic_bytes
     import ctypes as C
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    need = a.warmup + a.steps + a.profile_steps
+    pre = max(a.warmup, FIRST_TIMED_STEP - 1 - a.profile_steps)     # untimed steps before the profile window
+    need = pre + a.profile_steps + a.steps
     T_run = max(wl.T, (need + 1) * wl.dt)
     sim = make_sim(wl, dev, T=T_run)
     sim.assemble()
@@ -207,12 +246,14 @@ def tcb_arm(a, wl, world, rank, local):
     sim._setup(1e-5, 1e-5, 100, True, True, 1.0, keep_snapshots=False)
     stream = torch.cuda.current_stream(dev)
     sim.run_steps(a.warmup)
+    tuned = sim.autotune()                        # launch shapes for this device and shape (cached)
+    sim.run_steps(pre - a.warmup)
     torch.cuda.synchronize(dev)
     lib = _lib.load()
     st = sim._sim["struct"]
     _lib.check(lib.tcb_mono_check(C.byref(st), stream.cuda_stream))
     cg_name = "cg_resident_kernel" if lib.tcb_mono_cg_kernel(C.byref(st)) == 1 else "cg_kernel"
-    # per-kernel event times for the roofline: steps warmup+1 .. warmup+profile_steps,
+    # per-kernel event times for the roofline: steps pre+1 .. pre+profile_steps,
     # each kernel bracketed by events on the launch stream (the same steps every run,
     # so an ncu capture of them measures the same launches)
     msi, msc = C.c_double(0.0), C.c_double(0.0)
@@ -230,22 +271,22 @@ def tcb_arm(a, wl, world, rank, local):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        done = 0
-        if replay:
-            for _ in range(a.steps // G):
-                replay()
-            done = (a.steps // G) * G
-        if a.steps > done:
-            sim.run_steps(a.steps - done)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
+    t_first = sim._sim["next_step"]
+    clk.mark("headline")
+    e0.record(stream)
+    done = 0
+    if replay:
+        for _ in range(a.steps // G):
+            replay()
+        done = (a.steps // G) * G
+    if a.steps > done:
+        sim.run_steps(a.steps - done)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
     del replay
     ms = replicas.reduce_max(e0.elapsed_time(e1))     # slowest rank (replicas only)
     _lib.check(lib.tcb_mono_check(C.byref(st), stream.cuda_stream))
-    t0s = a.warmup + a.profile_steps
-    iters = sim._sim["step_iters"][t0s + 1: t0s + a.steps + 1].sum().item()
+    iters = sim._sim["step_iters"][t_first: t_first + a.steps].sum().item()
     k_loop = iters / a.steps + 1.0                    # CG loop passes per step (n_iter + 1)
     b_ion, b_rhs, b_iter = algorithmic_bytes(sys_.n, sys_.nnz, sim.ionic_model.state.shape[0])
     t_ion = msi.value / a.profile_steps * 1e-3
@@ -267,11 +308,35 @@ def tcb_arm(a, wl, world, rank, local):
     del sim
     torch.cuda.empty_cache()
 
+    # the whole run of the workload (T = 100 ms, every step), timed on the device
+    full = None
+    if not a.no_full_run:
+        simf = make_sim(wl, dev)
+        simf.assemble()
+        simf._setup(1e-5, 1e-5, 100, True, True, 1.0, keep_snapshots=False)
+        simf.autotune()
+        torch.cuda.synchronize(dev)
+        clk.mark("full_run")
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        simf._advance(wl.nt, 100)
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        fms = replicas.reduce_max(f0.elapsed_time(f1))
+        f_iters = simf._sim["step_iters"][1: wl.nt + 1].sum().item()
+        full = {"value": world * wl.n_nodes * wl.nt / (fms / 1e3), "unit": METRIC, "steps": wl.nt,
+                "ms_per_step": fms / wl.nt, "cg_iterations_per_step": f_iters / wl.nt,
+                "what": "every step 1..nt of the workload on the device (CUDA events; replays of 100-step "
+                        "graphs after one plain step), no set-up or download"}
+        del simf
+        torch.cuda.empty_cache()
+
     # e2e: one full solve of the workload through the public API from host arrays
     e2e = None
     if not a.no_e2e:
         if world > 1:
             torch.distributed.barrier()
+        clk.mark("e2e")
         with tempfile.TemporaryDirectory() as d:
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
@@ -280,6 +345,7 @@ def tcb_arm(a, wl, world, rank, local):
                        verbose=False, result_path=d)
             torch.cuda.synchronize(dev)
             wall = time.perf_counter() - t0
+            e_iters = int(sim2.n_total_iter)
             h2d = (wl.nodes_mm.size * 4 + wl.elems.size * 4 + wl.regions.size * 4 + wl.fibres.size * 4 +
                    wl.n_nodes * 4 + (wl.nt + 1) * 8)
             d2h = 2 * wl.n_nodes * 4 + (wl.nt // int(1.0 / wl.dt) + 1) * wl.n_nodes * 4 + (wl.nt + 1) * 4
@@ -287,52 +353,61 @@ def tcb_arm(a, wl, world, rank, local):
         wall = replicas.reduce_max(wall)
         e2e = {"value": world * wl.n_nodes * wl.nt / wall, "unit": METRIC,
                "h2d_bytes_per_step": int(h2d // wl.nt), "d2h_bytes_per_step": int(d2h // wl.nt),
+               "cg_iterations_per_step": e_iters / wl.nt,
                "what": f"one Monodomain.solve of the workload (T={wl.T} ms, {wl.nt} steps) from host arrays: "
                        f"mesh upload, assembly, all steps, AT/RT/Vm download and save; wall {wall:.2f} s"}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        clk.mark(None)
         r = time_oracle(wl, budget_s=float(os.environ.get("TCB_CPU_BASELINE_S", "15")), min_steps=3, warmup=3)
         cpu = {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": "port",
                "sample": f"oracle on the full workload, {r['steps']} steps after an untimed "
                          f"{r['assemble_s']:.1f} s assembly and {r['warmup']} untimed warm-up steps "
                          f"({r['seconds']:.1f} s of stepping)"}
-    if rank != 0:
-        return
-    line = {
+    clk.mark(None)
+    shape = tuned.get("ionic_shape") or list(_lib.ionic_variants(st.model)[max(tuned["ionic_variant"], 1) - 1])
+    return {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": wl.name, "nodes": wl.n_nodes, "elements": int(len(wl.elems)), "nnz": sys_.nnz,
                    "dt_ms": wl.dt, "T_ms": wl.T, "parallelism": "replicas only" if world > 1 else "single",
-                   "cg_tol": 1e-5, "cg_iterations_per_step": iters / a.steps, "cuda_graph_steps": G,
-                   "l2": "inputs larger than L2 (per-step working set > 300 MB)",
-                   "simulated_ms_per_s": world * wl.dt * a.steps / (ms / 1e3)},
+                   "cg_tol": 1e-5, "timed_steps": [t_first, t_first + a.steps - 1],
+                   "untimed_steps_before": t_first - 1, "cg_iterations_per_step": iters / a.steps,
+                   "cuda_graph_steps": G, "l2": "inputs larger than L2 (per-step working set > 300 MB)",
+                   "simulated_ms_per_s": world * wl.dt * a.steps / (ms / 1e3),
+                   "tuned": {"ionic_variant": int(tuned["ionic_variant"]),
+                             "ionic_nodes_per_thread": int(shape[0]), "ionic_blocks_per_sm": int(shape[1]),
+                             "ionic_fast_math": int(shape[2]), "cg_blocks_per_sm": int(tuned["cg_per_sm"]),
+                             "source": "cache" if tuned.get("cached") else "measured"}},
         "gpu_launches": 2 * a.steps,
-        "clocks": clk.summary(),
         "roofline": {"bound": "hbm", "kernel": dominant[0], "achieved": dominant[1], "peak": peak,
                      "unit": "GB/s", "frac": dominant[1] / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} HBM copy bandwidth",
-                     "profile_steps": [a.warmup + 1, a.warmup + a.profile_steps],
+                     "profile_steps": [s0, s0 + a.profile_steps - 1],
                      "kernels": {cg_name: {"ms_per_launch": 1e3 * t_cg, "bytes": cg_bytes, "GB/s": gbs_cg,
                                            "cg_loop_passes": kp},
                                  "mono_ionic_kernel": {"ms_per_launch": 1e3 * t_ion, "bytes": b_ion,
                                                        "GB/s": gbs_ion}},
                      "step": {"bytes": step_bytes, "GB/s": step_bytes / (ms / a.steps * 1e-3) / 1e9}},
+        "full_run": full,
         "e2e": e2e,
         "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
 
 
-def batch_arm(a, world, rank, local):
-    """Batched mix (64 cubes, MS/TTP) vs the same simulations one at a time."""
+def batch_arm(a, world, rank, local, clk, steps=None):
+    """Batched mix (64 cubes, MS/TTP) vs the same simulations one at a time on the
+    single-simulation path, and a full batched run from host arrays.  Returns the
+    line (``--workload batch_cubes``) or the ``batch`` object of the default line."""
     from torchcor_b200.simulator import MonodomainBatch
-    from torchcor_b200.workloads import batch_cubes
+    from torchcor_b200.workloads import algorithmic_bytes, batch_cubes
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     wls = batch_cubes()
     total = sum(w.n_nodes for w in wls)
+    K = steps or a.steps
     stream = torch.cuda.current_stream(dev)
     batch = MonodomainBatch(dev)
     if a.cg_variant:
@@ -351,38 +426,36 @@ def batch_arm(a, world, rank, local):
         torch.cuda.synchronize(dev)
     cg_cfg = batch.cg_config
     # the timed steps replay CUDA graphs of G steps, the remainder runs as plain launches
-    G = a.graph_steps if 0 < a.graph_steps <= a.steps else 0
+    G = a.batch_graph_steps if 0 < a.batch_graph_steps <= K else 0
     replay = batch.capture(G) if G else None
     if replay:
         replay()
     torch.cuda.synchronize(dev)
+    first = batch.sims[0]._sim["next_step"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    K = a.steps
     if world > 1:
         torch.distributed.barrier()
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        done = 0
-        if replay:
-            for _ in range(K // G):
-                replay()
-            done = (K // G) * G
-        if K > done:
-            batch.step(K - done)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
+    clk.mark("batch")
+    e0.record(stream)
+    done = 0
+    if replay:
+        for _ in range(K // G):
+            replay()
+        done = (K // G) * G
+    if K > done:
+        batch.step(K - done)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk.mark(None)
     ms = replicas.reduce_max(e0.elapsed_time(e1))     # slowest rank (each rank runs the batch)
     batch.check()
-    iters = sum(int(s._sim["step_iters"].sum().item()) for s in batch.sims)
     # CG passes of the timed steps: the batch kernel runs max_i(it_i + 1) passes a
     # step; a node needs only its own simulation's it_i + 1
-    lo, hi = a.warmup + 1, a.warmup + K + (G if G else 0)
-    its = torch.stack([s._sim["step_iters"][lo:hi + 1].long() for s in batch.sims])
+    its = torch.stack([s._sim["step_iters"][first:first + K].long() for s in batch.sims])
     sizes = torch.tensor([s._sim["struct"].n_nodes for s in batch.sims], device=its.device, dtype=torch.float64)
     passes_max = float((its.max(0).values + 1).double().mean().item())
-    passes_node = float(((its + 1).double() * sizes[:, None]).sum().item() / (sizes.sum().item() * its.shape[1]))
+    passes_node = float(((its + 1).double() * sizes[:, None]).sum().item() / (sizes.sum().item() * K))
     # algorithmic bytes of the timed steps (each simulation's B_ion + B_rhs + (it+1) B_iter)
-    from torchcor_b200.workloads import algorithmic_bytes
     step_bytes = 0.0
     for k, s_ in enumerate(batch.sims):
         bi, br, bt = algorithmic_bytes(s_.system.n, s_.system.nnz, s_.ionic_model.state.shape[0])
@@ -391,49 +464,77 @@ def batch_arm(a, world, rank, local):
     value = world * total * K / (ms / 1e3)
     del batch, replay
     torch.cuda.empty_cache()
-    # the plain single-simulation path on the same simulations, one after the other
+    # the plain single-simulation path on the same simulations over the same steps,
+    # one after the other
     plain_ms = 0.0
     if not a.no_plain:
         for w in wls:
             sim = make_sim(w, dev)
             sim.prepare(1e-5, 1e-5, 100, snapshot_interval=w.T)
-            sim.run_steps(a.warmup)
+            sim.autotune()
+            sim.run_steps(first - 1)
             torch.cuda.synchronize(dev)
+            clk.mark("batch_plain")
             e0.record(stream)
             sim.run_steps(K)
             e1.record(stream)
             torch.cuda.synchronize(dev)
+            clk.mark(None)
             plain_ms += e0.elapsed_time(e1)
             del sim
     plain_ms = replicas.reduce_max(plain_ms)
     plain = world * total * K / (plain_ms / 1e3) if plain_ms else None
-    if rank != 0:
-        return
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": a.warmup,
-            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batch of {len(wls)} tet cubes (16..64 nodes per edge, h 0.25 mm), "
-                                   f"Mitchell-Schaeffer/TTP ENDO 50/50, dt 0.01 ms",
-                       "simulations": len(wls), "nodes": total, "cuda_graph_steps": G,
-                       "cg_variant": cg_cfg[0], "cg_blocks": cg_cfg[1],
-                       "autotune_ms_per_step": tuned,
-                       "cg_iterations_per_step": iters / max(1, (K + a.warmup + (G if G else 0))) / len(wls),
-                       "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,
-                       "setup_s": setup_s},
-            "gpu_launches": 3 * K, "clocks": clk.summary(),
-            "roofline": {"bound": "hbm", "kernel": "whole batch step (ionic per model + batched CG)",
-                         "achieved": step_bytes / (ms / K * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": step_bytes / (ms / K * 1e-3) / 1e9 / peak, "traffic": None,
-                         "peak_source": f"{peak_kind} HBM copy bandwidth", "bytes_per_step": step_bytes},
-            "plain_single_path": {"value": plain, "unit": METRIC,
-                                  "what": "each simulation alone through Monodomain (same steps), summed time"},
-            "speedup_vs_plain": (value / plain) if plain else None}
-    print(json.dumps(line), flush=True)
+    # e2e: every simulation built from host arrays, batched, run to its end, results on the host
+    e2e = None
+    if not a.no_e2e:
+        torch.cuda.synchronize(dev)
+        clk.mark("batch_e2e")
+        t0 = time.perf_counter()
+        b2 = MonodomainBatch(dev)
+        if a.cg_variant:
+            b2.set_cg(a.cg_variant)
+        sims = [b2.add(make_sim(w, dev), 1e-5, 1e-5, 100, snapshot_interval=w.T) for w in wls]
+        b2.autotune()
+        b2.run()
+        at = [s.activation_time.cpu() for s in sims]
+        torch.cuda.synchronize(dev)
+        wall = replicas.reduce_max(time.perf_counter() - t0)
+        clk.mark(None)
+        nt = wls[0].nt
+        h2d = sum(w.nodes_mm.size * 4 + w.elems.size * 4 + w.regions.size * 4 + w.fibres.size * 4 + w.n_nodes * 4
+                  for w in wls)
+        d2h = sum(2 * w.n_nodes * 4 + w.n_nodes * 4 for w in wls)
+        e2e = {"value": world * total * nt / wall, "unit": METRIC, "h2d_bytes_per_step": int(h2d // nt),
+               "d2h_bytes_per_step": int(d2h // nt), "activated_nodes": int(sum(int((x > 0).sum()) for x in at)),
+               "what": f"the {len(wls)} simulations built from host arrays, batched (MonodomainBatch.run), "
+                       f"every one run to T = {wls[0].T} ms ({nt} steps), AT/RT/Vm downloaded; wall {wall:.2f} s"}
+        del b2, sims
+        torch.cuda.empty_cache()
+    out = {"metric": METRIC, "value": value, "unit": METRIC, "steps": K, "ms_per_step": ms / K,
+           "timed_steps": [first, first + K - 1], "cuda_graph_steps": G,
+           "config": {"workload": f"batch of {len(wls)} tet cubes (16..64 nodes per edge, h 0.25 mm), "
+                                  f"Mitchell-Schaeffer/TTP ENDO 50/50, dt 0.01 ms",
+                      "simulations": len(wls), "nodes": total, "cg_variant": cg_cfg[0], "cg_blocks": cg_cfg[1],
+                      "autotune_ms_per_step": tuned, "cg_iterations_per_step":
+                          float(its.sum().item()) / K / len(wls),
+                      "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,
+                      "setup_s": setup_s},
+           "gpu_launches": 2 * K,
+           "roofline": {"bound": "hbm", "kernel": "whole batch step (one ionic launch + one batched CG launch)",
+                        "achieved": step_bytes / (ms / K * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": step_bytes / (ms / K * 1e-3) / 1e9 / peak, "traffic": None,
+                        "peak_source": f"{peak_kind} HBM copy bandwidth", "bytes_per_step": step_bytes},
+           "plain_single_path": {"value": plain, "unit": METRIC,
+                                 "what": "each simulation alone through Monodomain (tuned launch shapes, same "
+                                         "steps), summed device time"},
+           "speedup_vs_plain": (value / plain) if plain else None,
+           "e2e": e2e}
+    return out
 
 
-def serving_arm(a, world, rank, local):
-    """Request stream served on one GPU per rank (independent replicas); prints
-    throughput and p50/p99 request latency."""
+def serving_arm(a, world, rank, local, clk):
+    """Request stream served on one GPU per rank (independent replicas): throughput
+    and p50/p99 request latency."""
     from torchcor_b200 import serving
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -441,22 +542,27 @@ def serving_arm(a, world, rank, local):
     server = serving.Server(dev)
     if world > 1:
         torch.distributed.barrier()
-    with ClockSampler(local) as clk:
-        summ = server.run(reqs)
+    clk.mark("serving")
+    summ = server.run(reqs)
+    clk.mark(None)
     # each rank serves its own stream: whole-job rate = all ranks' node-steps / slowest wall
     total_ns = replicas.reduce_sum(summ["node_steps"])
     wall = replicas.reduce_max(summ["wall_s"])
-    if rank != 0:
-        return
-    line = {"metric": METRIC, "value": total_ns / wall, "unit": METRIC, "n_gpus": world,
-            "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+    return {"metric": METRIC, "value": total_ns / wall, "unit": METRIC,
             "config": {"workload": f"serving: {a.requests} requests, Poisson arrivals offered at {a.load} x "
                                    f"{a.capacity:.3g} node-steps/s, N lognormal(median 50k) in [10k, 500k], "
                                    f"cube/icosphere 50/50, MS/TTP/CRN, T U(50,300) ms, dt 0.01 ms",
                        "parallelism": "replicas only"},
-            "serving": summ, "gpu_launches": None, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+            "serving": summ}
+
+
+def standalone_line(obj, a, world):
+    """A batch or serving object as a line of its own (--workload batch_cubes|serving)."""
+    line = {"metric": METRIC, "value": obj["value"], "unit": METRIC, "n_gpus": world, "steps": obj.get("steps"),
+            "warmup": a.warmup, "ms_per_step": obj.get("ms_per_step"), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+    line.update({k: v for k, v in obj.items() if k not in line})
+    return line
 
 
 def main():
@@ -466,41 +572,52 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="tcb", choices=["tcb", "reference"])
     ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube", "batch_cubes", "serving"])
-    ap.add_argument("--requests", type=int, default=512, help="serving mode: requests in the stream")
-    ap.add_argument("--load", type=float, default=0.9, help="serving mode: offered load / capacity")
+    ap.add_argument("--requests", type=int, default=128, help="serving: requests in the stream")
+    ap.add_argument("--load", type=float, default=0.9, help="serving: offered load / capacity")
     ap.add_argument("--capacity", type=float, default=3.5e9,
-                    help="serving mode: node-steps/s the arrival rate assumes (measured for this mix)")
-    ap.add_argument("--graph-steps", type=int, default=-1,
-                    help="steps per captured CUDA graph in the timed region (0 = plain launches; "
-                         "default 100 for a single simulation, 50 for a batch)")
-    ap.add_argument("--no-plain", action="store_true", help="batch mode: skip the one-at-a-time comparison")
+                    help="serving: node-steps/s the arrival rate assumes (measured for this mix)")
+    ap.add_argument("--graph-steps", type=int, default=100,
+                    help="steps per captured CUDA graph in the timed region (0 = plain launches)")
+    ap.add_argument("--batch-graph-steps", type=int, default=50)
+    ap.add_argument("--batch-steps", type=int, default=200, help="timed batch steps in the default line")
+    ap.add_argument("--no-plain", action="store_true", help="batch: skip the one-at-a-time comparison")
     ap.add_argument("--cg-variant", type=int, default=0, choices=[0, 1, 2, 3],
-                    help="batch mode: batched CG variant (1/2 streaming, 3 staged); 0 = autotuned")
+                    help="batch: batched CG variant (1/2 streaming, 3 staged); 0 = autotuned")
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-full-run", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="default line without the batch object")
+    ap.add_argument("--no-serving", action="store_true", help="default line without the serving object")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be at least 3")
-    if a.graph_steps < 0:
-        a.graph_steps = 50 if a.workload == "batch_cubes" else 100
     from torchcor_b200.workloads import WORKLOADS
     world, rank, local = dist_setup(a.impl)
-    if a.workload == "serving":
-        serving_arm(a, world, rank, local)
-        if world > 1:
-            torch.distributed.destroy_process_group()
-        return
-    if a.workload == "batch_cubes":
-        batch_arm(a, world, rank, local)
-        if world > 1:
-            torch.distributed.destroy_process_group()
-        return
-    wl = WORKLOADS[a.workload]()
     if a.impl == "reference":
-        reference_arm(a, wl, world, rank)
+        if a.workload in WORKLOADS:
+            reference_arm(a, WORKLOADS[a.workload](), world, rank)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the single-simulation "
+                              "workloads (ttp_cube, ms_cube); the reference has no batched or served path"}))
         return
-    tcb_arm(a, wl, world, rank, local)
+    clk = ClockSampler(local)
+    try:
+        if a.workload == "serving":
+            line = standalone_line(serving_arm(a, world, rank, local, clk), a, world)
+        elif a.workload == "batch_cubes":
+            line = standalone_line(batch_arm(a, world, rank, local, clk), a, world)
+        else:
+            line = tcb_arm(a, WORKLOADS[a.workload](), world, rank, local, clk)
+            if a.workload == "ttp_cube" and not a.no_batch:
+                line["batch"] = batch_arm(a, world, rank, local, clk, steps=a.batch_steps)
+            if a.workload == "ttp_cube" and not a.no_serving:
+                line["serving"] = serving_arm(a, world, rank, local, clk)
+    finally:
+        clk.stop()
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
 

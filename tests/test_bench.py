@@ -28,3 +28,17 @@ def test_reference_arm_line():
     assert line["e2e"] == {"value": line["value"], "unit": "node-steps/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] and line["config"]["nodes"] == 9261
+
+
+def test_clock_sampler_counts_marked_segments_only():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    c = bench.ClockSampler(0)
+    c.proc = False                                   # no nvidia-smi here: feed samples by hand
+    line = "0, {}, 1965, 500, 0x0, Not Active, Not Active, Not Active, {}"
+    c.segments = [["headline", 1.0, 2.0], ["e2e", 3.0, 4.0]]
+    c.samples = [(0.5, line.format(300, "Not Active")), (1.5, line.format(1965, "Not Active")),
+                 (2.5, line.format(300, "Not Active")), (3.5, line.format(1900, "Active"))]
+    s = c.summary()
+    assert s["samples"] == 2 and s["sm_mhz"] == (1965 + 1900) / 2 and s["sm_max_mhz"] == 1965
+    assert s["reasons"] == ["sw_power_cap"] and set(s["segments"]) == {"headline", "e2e"}
