@@ -252,7 +252,9 @@ def tcb_arm(a, wl, world, rank, local, clk):
     lib = _lib.load()
     st = sim._sim["struct"]
     _lib.check(lib.tcb_mono_check(C.byref(st), stream.cuda_stream))
-    cg_name = "cg_resident_kernel" if lib.tcb_mono_cg_kernel(C.byref(st)) == 1 else "cg_kernel"
+    kind = lib.tcb_mono_cg_kernel(C.byref(st))
+    fused = kind == 2
+    cg_name = {2: "cg_resident_kernel (fused step)", 1: "cg_resident_kernel", 0: "cg_kernel"}[kind]
     # per-kernel event times for the roofline: steps pre+1 .. pre+profile_steps,
     # each kernel bracketed by events on the launch stream (the same steps every run,
     # so an ncu capture of them measures the same launches)
@@ -292,12 +294,15 @@ def tcb_arm(a, wl, world, rank, local, clk):
     t_ion = msi.value / a.profile_steps * 1e-3
     t_cg = msc.value / a.profile_steps * 1e-3
     peak, peak_kind = peaks()
-    cg_bytes = b_rhs + kp * b_iter
+    cg_bytes = b_rhs + kp * b_iter + (b_ion if fused else 0)
     gbs_cg = cg_bytes / t_cg / 1e9
-    gbs_ion = b_ion / t_ion / 1e9
+    gbs_ion = b_ion / t_ion / 1e9 if t_ion > 0 else None
     step_bytes = b_ion + b_rhs + k_loop * b_iter
     value = world * wl.n_nodes * a.steps / (ms / 1e3)
     dominant = (cg_name, gbs_cg, cg_bytes) if t_cg >= t_ion else ("mono_ionic_kernel", gbs_ion, b_ion)
+    kernels = {cg_name: {"ms_per_launch": 1e3 * t_cg, "bytes": cg_bytes, "GB/s": gbs_cg, "cg_loop_passes": kp}}
+    if not fused:
+        kernels["mono_ionic_kernel"] = {"ms_per_launch": 1e3 * t_ion, "bytes": b_ion, "GB/s": gbs_ion}
     # DRAM traffic per launch of the dominant kernel over the same profile steps,
     # from an ncu capture (profiles/traffic.json; the capture command is stored there)
     traffic = None
@@ -380,16 +385,14 @@ def tcb_arm(a, wl, world, rank, local, clk):
                    "tuned": {"ionic_variant": int(tuned["ionic_variant"]),
                              "ionic_nodes_per_thread": int(shape[0]), "ionic_blocks_per_sm": int(shape[1]),
                              "ionic_fast_math": int(shape[2]), "cg_blocks_per_sm": int(tuned["cg_per_sm"]),
+                             "fused_step": int(tuned.get("fused_step", 0)),
                              "source": "cache" if tuned.get("cached") else "measured"}},
-        "gpu_launches": 2 * a.steps,
+        "gpu_launches": (1 if fused else 2) * a.steps,
         "roofline": {"bound": "hbm", "kernel": dominant[0], "achieved": dominant[1], "peak": peak,
                      "unit": "GB/s", "frac": dominant[1] / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} HBM copy bandwidth",
                      "profile_steps": [s0, s0 + a.profile_steps - 1],
-                     "kernels": {cg_name: {"ms_per_launch": 1e3 * t_cg, "bytes": cg_bytes, "GB/s": gbs_cg,
-                                           "cg_loop_passes": kp},
-                                 "mono_ionic_kernel": {"ms_per_launch": 1e3 * t_ion, "bytes": b_ion,
-                                                       "GB/s": gbs_ion}},
+                     "kernels": kernels,
                      "step": {"bytes": step_bytes, "GB/s": step_bytes / (ms / a.steps * 1e-3) / 1e9}},
         "full_run": full,
         "e2e": e2e,

@@ -207,6 +207,10 @@ typedef struct tcb_mono {
                                 and stim_bits aligned to the vector (else the first one-node instance runs) */
     int32_t cg_per_sm;       /* blocks per SM of the CG kernel that keeps rows in shared memory: 0 = the
                                 most whose rows fit (2, else 1); 1 or 2 pins it */
+    int32_t fused_step;      /* 1: each step is one launch, the ionic update fused into the CG kernel that
+                                keeps rows in shared memory (where that kernel applies: int16 column
+                                offsets, rows that fit); 0: the ionic and CG kernels as two launches.
+                                The values are the same either way */
     /* device bookkeeping (caller-allocated, zero-initialised) */
     int32_t* step_iters;     /* [nt+1] CG iterations of each step */
     int32_t* counter;        /* [4]: next step, error code, 2 spare */
@@ -230,11 +234,13 @@ int tcb_mono_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* 
 int tcb_mono_cg_run(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream);
 /* Like tcb_mono_run, recording CUDA events around every kernel on `stream`;
  * adds the summed device times (ms) of the ionic and CG kernels to
- * ms_ionic / ms_cg (for roofline accounting; costs one event pair per launch). */
+ * ms_ionic / ms_cg (for roofline accounting; costs one event pair per launch).
+ * A fused step's single kernel counts as CG time (ms_ionic gets nothing). */
 int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t step_end, void* stream, double* ms_ionic,
                      double* ms_cg);
 /* Which CG kernel tcb_mono_run launches for this simulation on the current
- * device: 1 = the kernel keeping each block's rows in shared memory, 0 = the
+ * device: 2 = the fused step (ionic update inside the CG kernel that keeps rows
+ * in shared memory), 1 = that CG kernel after a separate ionic launch, 0 = the
  * streaming kernel; negative = error status.  No counterpart in the reference
  * (used to label measurements). */
 int tcb_mono_cg_kernel(const tcb_mono* m);

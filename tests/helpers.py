@@ -48,7 +48,7 @@ def run_oracle_tissue(case, mesh_dir, **kw):
     return sim, sim.solve(case["tol"], case["tol"], case["max_iter"], **kw)
 
 
-def run_device_tissue(case, mesh_dir, device, result_dir=None):
+def run_device_tissue(case, mesh_dir, device, result_dir=None, launch=None):
     from torchcor_b200.simulator import Monodomain
     sim = Monodomain(device_ionic(case, device), T=case["T"], dt=case["dt"], device=device)
     sim.load_mesh(mesh_dir)
@@ -58,7 +58,7 @@ def run_device_tissue(case, mesh_dir, device, result_dir=None):
         sim.add_stimulus(str(Path(mesh_dir) / s["file"]), start=s["start"], duration=s["duration"],
                          intensity=s["intensity"], period=s.get("period"), count=s.get("count", 1))
     total = sim.solve(a_tol=case["tol"], r_tol=case["tol"], max_iter=case["max_iter"], calculate_AT_RT=True,
-                      linear_guess=True, snapshot_interval=1, verbose=False, result_path=result_dir)
+                      linear_guess=True, snapshot_interval=1, verbose=False, result_path=result_dir, launch=launch)
     return sim, total
 
 

@@ -142,11 +142,11 @@ TISSUE = ["cube6_ms_f32", "cfg1_ms_f32", "cube8_ttp_f32", "ico3_crn_f32", "cube4
 
 
 @pytest.mark.parametrize("name", TISSUE)
-def test_monodomain_matches_reference(lib, cuda, name, tmp_path):
+def test_monodomain_matches_reference(lib, cuda, name, tmp_path, launch=None):
     case = C.case(name)
     g = golden(name)
     out = tmp_path / "out"
-    sim, total = run_device_tissue(case, case_mesh_dir(case, tmp_path), cuda, result_dir=out)
+    sim, total = run_device_tissue(case, case_mesh_dir(case, tmp_path), cuda, result_dir=out, launch=launch)
     AT = torch.load(out / "ATs.pt").numpy()
     RT = torch.load(out / "RTs.pt").numpy()
     Vm = torch.load(out / "Vm.pt").numpy()
@@ -161,6 +161,13 @@ def test_monodomain_matches_reference(lib, cuda, name, tmp_path):
     assert err <= 1e-3, err
     ref_total = int(g["n_total_iter"])
     assert abs(total - ref_total) <= max(3, ref_total // 50), (total, ref_total)
+
+
+@pytest.mark.parametrize("fused", [0, 1])
+@pytest.mark.parametrize("name", TISSUE)
+def test_monodomain_step_launches(lib, cuda, name, tmp_path, fused):
+    """The step as two launches and as one fused launch, both against the reference."""
+    test_monodomain_matches_reference(lib, cuda, name, tmp_path, launch=dict(fused_step=fused))
 
 
 @pytest.mark.parametrize("variant", [dict(TCB_CG_KERNEL="streaming"), dict(TCB_CG_INDEX="int32")])

@@ -74,3 +74,27 @@ def test_tuner_sets_and_caches_its_choice(lib, cuda, tmp_path):
     assert again.get("cached") and again["ionic_variant"] == got["ionic_variant"]
     total = sim.solve(case["tol"], case["tol"], case["max_iter"], verbose=False, autotune=False)
     assert total > 0
+
+
+@pytest.mark.parametrize("name", ["cube6_ms_f32", "cube8_ttp_f32", "ico3_crn_f32"])
+def test_fused_step_equals_two_launches(lib, cuda, tmp_path, name):
+    """The step as one launch (ionic update inside the resident CG kernel) gives the
+    two-launch step's values bit for bit: same sums in the same order."""
+    from torchcor_b200 import _lib
+    case = CS.case(name)
+    d = case_mesh_dir(case, tmp_path)
+    sims = [_prepared(case, d, cuda) for _ in range(2)]
+    for sim, fused in zip(sims, (0, 1)):
+        sim.set_launch(ionic_variant=1, cg_per_sm=0, fused_step=fused)
+    st = [s._sim["struct"] for s in sims]
+    assert lib.tcb_mono_cg_kernel(C.byref(st[0])) == 1 and lib.tcb_mono_cg_kernel(C.byref(st[1])) == 2
+    nt = sims[0].nt
+    for sim, m in zip(sims, st):
+        _lib.check(lib.tcb_mono_run(C.byref(m), 1, nt + 1, _lib.stream_ptr()))
+        _lib.check(lib.tcb_mono_check(C.byref(m), _lib.stream_ptr()))
+    a, b = (s._sim for s in sims)
+    assert torch.equal(a["step_iters"], b["step_iters"])
+    # instance 1 of each model and its fused step share the division policy
+    for key in ("x", "at_rt"):
+        assert torch.equal(a[key], b[key]), key
+    assert torch.equal(sims[0].ionic_model.state, sims[1].ionic_model.state)

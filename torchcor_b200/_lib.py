@@ -45,6 +45,7 @@ class tcb_mono(C.Structure):
         ("a_tol", _f64), ("r_tol", _f64),
         ("max_iter", _i32), ("linear_guess", _i32), ("at_rt", _i32), ("per_frame", _i32), ("a_split", _i32),
         ("cm", C.c_float), ("dt", C.c_float), ("snap_ring", _i32), ("ionic_variant", _i32), ("cg_per_sm", _i32),
+        ("fused_step", _i32),
         ("step_iters", _vp), ("counter", _vp), ("scratch", _vp), ("barrier", _vp),
         ("params", _vp),
     ]

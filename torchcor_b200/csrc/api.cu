@@ -147,7 +147,13 @@ extern "C" int tcb_mono_run(const tcb_mono* m, int64_t step_begin, int64_t step_
         return fail(TCB_EINVAL, "tcb_mono_run: step range outside [1, nt]");
     cudaStream_t s = as_stream(stream);
     MonoDev d = make_dev(m);
+    const bool fused = step_begin < step_end && uses_fused_step(m, d);
     for (int64_t n = step_begin; n < step_end; ++n) {
+        if (fused) {
+            st = launch_mono_step(m, d, s);
+            if (st < 0) return st;
+            if (st == 1) continue;
+        }
         st = launch_mono_ionic(m, d, s);
         if (st) return st;
         st = launch_cg(d, s);
@@ -184,12 +190,20 @@ extern "C" int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t s
     std::vector<cudaEvent_t> ev(3 * count);
     for (auto& e : ev) TCB_CHECK_CUDA(cudaEventCreate(&e));
     int rc = TCB_OK;
+    const bool fused = uses_fused_step(m, d);
     for (int64_t i = 0; i < count && rc == TCB_OK; ++i) {
         cudaEventRecord(ev[3 * i], s);
-        rc = launch_mono_ionic(m, d, s);
-        if (rc) break;
+        if (!fused) {
+            rc = launch_mono_ionic(m, d, s);
+            if (rc) break;
+        }
         cudaEventRecord(ev[3 * i + 1], s);
-        rc = launch_cg(d, s);
+        if (fused) {
+            rc = launch_mono_step(m, d, s);
+            rc = rc == 1 ? TCB_OK : rc < 0 ? rc : fail(TCB_EINVAL, "fused step not applicable");
+        } else {
+            rc = launch_cg(d, s);
+        }
         cudaEventRecord(ev[3 * i + 2], s);
     }
     if (rc == TCB_OK) {
@@ -210,7 +224,9 @@ extern "C" int tcb_mono_profile(const tcb_mono* m, int64_t step_begin, int64_t s
 extern "C" int tcb_mono_cg_kernel(const tcb_mono* m) {
     int st = validate(m);
     if (st) return st;
-    return cg_uses_resident(make_dev(m)) ? 1 : 0;
+    const MonoDev d = make_dev(m);
+    if (uses_fused_step(m, d)) return 2;
+    return cg_uses_resident(d) ? 1 : 0;
 }
 
 extern "C" int tcb_mono_finish(const tcb_mono* m, void* stream) {

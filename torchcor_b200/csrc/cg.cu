@@ -193,6 +193,9 @@ int cg_blocks(const MonoDev& d) {
     return (int)(nb < 1 ? 1 : nb);
 }
 
+// the test variables that force the streaming kernel or 32-bit columns (these also rule out the fused step)
+bool cg_forced_fallback() { return env_is("TCB_CG_KERNEL", "streaming") || env_is("TCB_CG_INDEX", "int32"); }
+
 // 1 if launch_cg runs the shared-memory-resident kernel for this simulation, 0 if the streaming one
 int cg_uses_resident(const MonoDev& d) { return !env_is("TCB_CG_KERNEL", "streaming") && resident_blocks(d) > 0; }
 

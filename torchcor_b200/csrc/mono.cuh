@@ -52,6 +52,13 @@ int launch_mono_finish(const MonoDev& d, cudaStream_t s);
 int launch_cg(const MonoDev& d, cudaStream_t s);
 int launch_cg_resident(const MonoDev& d, cudaStream_t s);
 int resident_blocks(const MonoDev& d);
+int launch_mono_step(const tcb_mono* m, const MonoDev& d, cudaStream_t s);   // 1 launched, 0 not applicable
+int mono_step_fusable(const tcb_mono* m, const MonoDev& d);
+bool cg_forced_fallback();
+// 1 if tcb_mono_run runs this simulation's steps as the fused kernel
+inline int uses_fused_step(const tcb_mono* m, const MonoDev& d) {
+    return m->fused_step && !cg_forced_fallback() && mono_step_fusable(m, d);
+}
 int cg_uses_resident(const MonoDev& d);
 
 }  // namespace tcb

@@ -468,6 +468,17 @@ class Monodomain:
         return self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval,
                            snapshot_interval < self.T)
 
+    def set_launch(self, ionic_variant=None, cg_per_sm=None, fused_step=None):
+        """Set the prepared simulation's launch shapes: ionic kernel instance (1..,
+        0 = default), CG blocks per SM (0, 1, 2), fused step (0 or 1)."""
+        m = self._sim["struct"]
+        if ionic_variant is not None:
+            m.ionic_variant = int(ionic_variant)
+        if cg_per_sm is not None:
+            m.cg_per_sm = int(cg_per_sm)
+        if fused_step is not None:
+            m.fused_step = int(fused_step)
+
     def autotune(self, steps=5, force=False):
         """Choose the launch shapes of the prepared simulation's kernels (ionic
         kernel instance, CG blocks per SM): the cached choice for this device and
@@ -478,7 +489,7 @@ class Monodomain:
         return self.tuned
 
     def solve(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1,
-              verbose=True, result_path=None, snapshot_ring=None, graph_steps=100, autotune=True):
+              verbose=True, result_path=None, snapshot_ring=None, graph_steps=100, autotune=True, launch=None):
         """monodomain.py:141-226.  ``snapshot_ring=R`` keeps only R snapshot frames on
         the device and streams every frame, as soon as it is written, into a pinned host
         tensor on a separate stream (``solutions`` is then that host tensor); the
@@ -486,7 +497,9 @@ class Monodomain:
         ``graph_steps=G`` runs every whole G-step stretch of the loop as the replay of
         one CUDA graph of the same kernels (recorded once per solve); the results are
         bit-identical to plain launches (``graph_steps=0``).  ``autotune`` picks the
-        kernels' launch shapes first (``autotune()``; cached per device and shape)."""
+        kernels' launch shapes first (``autotune()``; cached per device and shape);
+        ``launch`` (a dict of ``ionic_variant``, ``cg_per_sm``, ``fused_step``) sets
+        them explicitly instead."""
         self.result_path = Path(result_path) if result_path is not None else None
         if self.result_path is not None:
             self.result_path.mkdir(parents=True, exist_ok=True)
@@ -496,7 +509,9 @@ class Monodomain:
             raise ValueError("snapshot_ring must be a positive number of frames")
         sim = self._setup(a_tol, r_tol, max_iter, calculate_AT_RT, linear_guess, snapshot_interval, keep,
                           snapshot_ring or 0)
-        if autotune:
+        if launch:
+            self.set_launch(**launch)
+        elif autotune:
             self.autotune()
         t0 = time.time()
         ring = sim["ring"]

@@ -1,9 +1,10 @@
 """Autotuning of launch choices, with the choices cached on disk.
 
-Single simulations (``tune_single``): the instance of the fused ionic kernel
-(1, 2 or 4 consecutive nodes per thread, each compiled for a register budget
-of some blocks per SM; ``_lib.ionic_variants``) and the blocks per SM of the
-CG kernel that keeps rows in shared memory (1 or 2, where the rows fit).  Each
+Single simulations (``tune_single``): the instance of the ionic kernel (1, 2
+or 4 consecutive nodes per thread, each compiled for a register budget of some
+blocks per SM and a division policy; ``_lib.ionic_variants``), the blocks per SM
+of the CG kernel that keeps rows in shared memory (1 or 2, where the rows fit),
+and whether a step runs as two launches or as the fused one.  Each
 candidate is timed with CUDA events on a scratch copy of the simulation's
 mutable device buffers, from the simulation's current step, so the simulation
 itself is untouched; the key is the device, the model and log2 buckets of the
@@ -195,10 +196,12 @@ def tune_single(sim, steps=5, cache=None, force=False):
     shapes = _lib.ionic_variants(model.model_id)
     if hit is not None and 0 <= int(hit.get("ionic_variant", 0)) <= len(shapes):
         m.ionic_variant, m.cg_per_sm = int(hit["ionic_variant"]), int(hit.get("cg_per_sm", 0))
+        m.fused_step = int(hit.get("fused_step", 0))
         return dict(hit, cached=True)
     first = d["next_step"]
     if sim.nt + 1 - first < steps + 1:
-        return {"ionic_variant": int(m.ionic_variant), "cg_per_sm": int(m.cg_per_sm), "measured": False}
+        return {"ionic_variant": int(m.ionic_variant), "cg_per_sm": int(m.cg_per_sm),
+                "fused_step": int(m.fused_step), "measured": False}
     stream = torch.cuda.current_stream(sim.device)
     scratch = ScratchSim(sim)
     t_ion = {}
@@ -206,17 +209,22 @@ def tune_single(sim, steps=5, cache=None, force=False):
         scratch.struct.ionic_variant, scratch.struct.cg_per_sm = k, 0
         t_ion[k] = time_steps(scratch, first, steps, stream)[0]
     best_ion = min(t_ion, key=t_ion.get)
-    t_cg = {}
+    # the step as two launches (ionic + CG) or as one (fused), for each CG blocks per SM
+    t_step = {}
     lib = _lib.load()
     for c in (2, 1):
-        scratch.struct.ionic_variant, scratch.struct.cg_per_sm = best_ion, c
-        if lib.tcb_mono_cg_kernel(C.byref(scratch.struct)) != 1:   # rows do not fit: streaming kernel
-            continue
-        t_cg[c] = time_steps(scratch, first, steps, stream)[1]
-    best_cg = min(t_cg, key=t_cg.get) if t_cg else 0
+        for fused in (0, 1):
+            st = scratch.struct
+            st.ionic_variant, st.cg_per_sm, st.fused_step = best_ion, c, fused
+            if lib.tcb_mono_cg_kernel(C.byref(st)) != (2 if fused else 1):   # not resident / not fusable
+                continue
+            ti, tc = time_steps(scratch, first, steps, stream)
+            t_step[(c, fused)] = ti + tc
+    best_cg, best_fused = min(t_step, key=t_step.get) if t_step else (0, 0)
     del scratch
-    m.ionic_variant, m.cg_per_sm = best_ion, best_cg
-    choice = {"ionic_variant": best_ion, "cg_per_sm": best_cg, "ionic_shape": list(shapes[best_ion - 1]),
-              "ionic_ms": {str(k): v for k, v in t_ion.items()}, "cg_ms": {str(k): v for k, v in t_cg.items()}}
+    m.ionic_variant, m.cg_per_sm, m.fused_step = best_ion, best_cg, best_fused
+    choice = {"ionic_variant": best_ion, "cg_per_sm": best_cg, "fused_step": best_fused,
+              "ionic_shape": list(shapes[best_ion - 1]), "ionic_ms": {str(k): v for k, v in t_ion.items()},
+              "step_ms": {f"cg{c}_fused{f}": v for (c, f), v in t_step.items()}}
     cache.put(key, choice)
     return dict(choice, measured=True)
