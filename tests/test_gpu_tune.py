@@ -77,24 +77,30 @@ def test_tuner_sets_and_caches_its_choice(lib, cuda, tmp_path):
 
 
 @pytest.mark.parametrize("name", ["cube6_ms_f32", "cube8_ttp_f32", "ico3_crn_f32"])
-def test_fused_step_equals_two_launches(lib, cuda, tmp_path, name):
-    """The step as one launch (ionic update inside the resident CG kernel) gives the
-    two-launch step's values bit for bit: same sums in the same order."""
-    from torchcor_b200 import _lib
+def test_fused_step_matches_two_launches(lib, cuda, tmp_path, name):
+    """The step as one launch (ionic update inside the resident CG kernel) against
+    the two-launch step, from the same state (step 31, in the upstroke) over 20
+    steps: the same sums in the same order, so the only differences are the
+    multiply-add contractions the compiler picks for the inlined ionic update in
+    each kernel (last bits of b'): solutions within 1e-5 of their range, the same
+    CG iteration counts."""
+    from torchcor_b200 import _lib, tune
     case = CS.case(name)
-    d = case_mesh_dir(case, tmp_path)
-    sims = [_prepared(case, d, cuda) for _ in range(2)]
-    for sim, fused in zip(sims, (0, 1)):
-        sim.set_launch(ionic_variant=1, cg_per_sm=0, fused_step=fused)
-    st = [s._sim["struct"] for s in sims]
-    assert lib.tcb_mono_cg_kernel(C.byref(st[0])) == 1 and lib.tcb_mono_cg_kernel(C.byref(st[1])) == 2
-    nt = sims[0].nt
-    for sim, m in zip(sims, st):
-        _lib.check(lib.tcb_mono_run(C.byref(m), 1, nt + 1, _lib.stream_ptr()))
-        _lib.check(lib.tcb_mono_check(C.byref(m), _lib.stream_ptr()))
-    a, b = (s._sim for s in sims)
+    sim = _prepared(case, case_mesh_dir(case, tmp_path), cuda)
+    stream = torch.cuda.current_stream(cuda)
+    _lib.check(lib.tcb_mono_run(C.byref(sim._sim["struct"]), 1, 31, stream.cuda_stream))
+    sim._sim["next_step"] = 31
+    scratch = tune.ScratchSim(sim)
+    out = []
+    for fused in (0, 1):
+        m = scratch.struct
+        m.ionic_variant, m.cg_per_sm, m.fused_step = 1, 0, fused
+        assert lib.tcb_mono_cg_kernel(C.byref(m)) == (2 if fused else 1)
+        tune.time_steps(scratch, 31, 20, stream)
+        out.append({k: scratch.buf[k].clone() for k in ("x", "at_rt", "step_iters", "state")})
+    a, b = out
     assert torch.equal(a["step_iters"], b["step_iters"])
-    # instance 1 of each model and its fused step share the division policy
-    for key in ("x", "at_rt"):
-        assert torch.equal(a[key], b[key]), key
-    assert torch.equal(sims[0].ionic_model.state, sims[1].ionic_model.state)
+    for k in ("x", "state"):
+        err = (a[k] - b[k]).abs().max().item() / a[k].abs().max().item()
+        assert err <= 1e-5, (k, err)
+    assert (a["at_rt"] - b["at_rt"]).abs().max().item() <= case["dt"] * 1.001
