@@ -58,13 +58,27 @@ def _steps(times, dt):
     return np.where(t < 0, -1, np.rint(t / dt)).astype(np.int64)
 
 
+LAUNCHES = ("tuned", "exact")
+
+
+def _launch(kind, model_id):
+    """Launch shapes of a run: the tuner's choice, or the first ionic instance with
+    IEEE division and logf (two launches a step)."""
+    from torchcor_b200 import _lib
+    if kind == "tuned":
+        return None
+    k = next(i for i, sh in enumerate(_lib.ionic_variants(model_id)) if sh[2] == 0)
+    return dict(ionic_variant=k + 1, fused_step=0)
+
+
 @pytest.fixture(scope="module")
 def runs(cuda):
-    """Device runs of the full-size cases (built once per module)."""
+    """Device runs of the full-size cases (built once per module), with the tuned
+    launch shapes and with the IEEE-division ionic instance."""
     from torchcor_b200 import meshgen
     from torchcor_b200.simulator import Monodomain
     out = {}
-    for name in ("cfg2_ttp_f32", "cfg3_crn_f32"):
+    for name, kind in ((n, k) for n in ("cfg2_ttp_f32", "cfg3_crn_f32") for k in LAUNCHES):
         case = C.case(name)
         nodes_um, elems, reg, fib = C.mesh_arrays(case)
         stims = [C.stimulus_nodes(case, s["nodes"], nodes_um) for s in case["stimuli"]]
@@ -75,9 +89,11 @@ def runs(cuda):
             sim.add_conductivity(**c)
         for s, region in zip(case["stimuli"], stims):
             sim.add_stimulus(None, s["start"], s["duration"], s["intensity"], region=region)
-        total = sim.solve(case["tol"], case["tol"], case["max_iter"], verbose=False, snapshot_interval=1)
+        total = sim.solve(case["tol"], case["tol"], case["max_iter"], verbose=False, snapshot_interval=1,
+                          launch=_launch(kind, sim.ionic_model.model_id))
         sy = sim.system
-        out[name] = dict(
+        out[(name, kind)] = dict(kind=kind, launch=[int(sim._sim["struct"].ionic_variant),
+                                                    int(sim._sim["struct"].fused_step)],
             case=case, total=int(total), iters=sim._sim["step_iters"][1:sim.nt + 1].cpu().numpy(),
             at=sim.activation_time.cpu().numpy(), rt=sim.repolarization_time.cpu().numpy(),
             vm=sim.solutions.cpu().numpy(), digest=_digest(sy.rowptr.cpu().numpy(), sy.col.cpu().numpy()),
@@ -119,7 +135,8 @@ def _compare(run, ref_name):
     errs["iters_total"] = run["total"]
     errs["iters_total_ref"] = int(g["n_total_iter"])
     errs["iters_steps_equal_frac"] = float((run["iters"] == g["iters"]).mean())
-    record_parity(case["name"], ref_name, **errs)
+    record_parity(case["name"] + "/" + run["kind"], ref_name, ionic_variant=run["launch"][0],
+                  fused_step=run["launch"][1], **errs)
     assert errs["at_max_steps"] <= 1 and errs["at_unmatched_before_end"] == 0, errs
     # repolarisation crosses -70 mV slowly, so ~1e-4 mV moves the crossing by a step:
     # within one step at all but 1e-4 of the repolarised nodes, two steps everywhere
@@ -132,9 +149,10 @@ def _compare(run, ref_name):
     return g, errs
 
 
+@pytest.mark.parametrize("kind", LAUNCHES)
 @pytest.mark.parametrize("name", ["cfg2_ttp_f32", "cfg3_crn_f32"])
-def test_fullsize_matches_reference_float32(lib, runs, name):
-    run = runs[name]
+def test_fullsize_matches_reference_float32(lib, runs, name, kind):
+    run = runs[(name, kind)]
     g, errs = _compare(run, name)
     assert run["digest"] == str(g["pattern_sha256"]) and run["nnz"] == int(g["nnz"])
     for got, key in ((run["m_sum"], "M_sum"), (run["k_abs"], "K_abs_sum"), (run["a_sum"], "A_sum")):
@@ -144,7 +162,8 @@ def test_fullsize_matches_reference_float32(lib, runs, name):
         assert errs["rt_set"] > 0.9 * len(run["rt"])          # and it repolarises
 
 
+@pytest.mark.parametrize("kind", LAUNCHES)
 @pytest.mark.parametrize("name,ref64", [("cfg2_ttp_f32", "cfg2_ttp_f64"), ("cfg3_crn_f32", "cfg3_crn_f64")])
-def test_fullsize_error_against_float64_reference(lib, runs, name, ref64):
+def test_fullsize_error_against_float64_reference(lib, runs, name, ref64, kind):
     """The float32 device path (float64 CG reductions) against the reference run in float64."""
-    _compare(runs[name], ref64)
+    _compare(runs[(name, kind)], ref64)
