@@ -12,8 +12,9 @@ itself produced (tests/golden/make_golden.py, compact format).
 Repolarisation times.  Vm falls through -70 mV slowly (about 1 mV/ms late in the
 CRN action potential), so a difference of 1e-4 mV moves the crossing by a step
 of 0.02 ms; the reference's own float32 run is a step away from its float64 run
-at many nodes.  RT is required within one step at all but 1e-4 of the
-repolarised nodes and within two steps everywhere; the counts are reported.
+at thousands of nodes.  RT is required within one step of the float64
+reference at every node, and within two steps of the float32 reference; the
+counts of nodes more than one step away are reported.
 
 Each is compared with the reference's float32 run and with its float64 run:
 CSR pattern digest equal; matrix sums within 1e-5; activation/repolarisation
@@ -139,9 +140,12 @@ def _compare(run, ref_name):
                   fused_step=run["launch"][1], **errs)
     assert errs["at_max_steps"] <= 1 and errs["at_unmatched_before_end"] == 0, errs
     # repolarisation crosses -70 mV slowly, so ~1e-4 mV moves the crossing by a step:
-    # within one step at all but 1e-4 of the repolarised nodes, two steps everywhere
-    assert errs["rt_max_steps"] <= 2 and errs["rt_over_one_step"] <= 1e-4 * max(errs["rt_set"], 1), errs
-    assert errs["rt_unmatched_before_end"] <= 1e-4 * max(errs["rt_set"], 1), errs
+    # within one step of the float64 reference at every node; the float32 reference is
+    # itself a step away from that at many nodes, so within two steps of it
+    if ref_name.endswith("_f64"):
+        assert errs["rt_max_steps"] <= 1 and errs["rt_unmatched_before_end"] == 0, errs
+    else:
+        assert errs["rt_max_steps"] <= 2 and errs["rt_unmatched_before_end"] <= 1e-4 * max(errs["rt_set"], 1), errs
     assert errs["vm_rel_outside_upstroke"] <= 1e-3 and errs["vm_rel"] <= 1e-2, errs
     assert errs["vm_absmax_rel"] <= 1e-3, errs
     ref_total = int(g["n_total_iter"])

@@ -99,6 +99,7 @@ def test_reference_float32_vs_float64_spread(base):
         x, y = a[k].astype(np.int64), b[k].astype(np.int64)
         both = (x >= 0) & (y >= 0)
         errs[k[:2].lower() + "_max_steps"] = int(np.abs(x[both] - y[both]).max()) if both.any() else 0
+        errs[k[:2].lower() + "_one_step_apart"] = int((np.abs(x[both] - y[both]) == 1).sum())
         errs[k[:2].lower() + "_unmatched"] = int(((x >= 0) != (y >= 0)).sum())
     errs["iters_total"], errs["iters_total_ref"] = int(a["n_total_iter"]), int(b["n_total_iter"])
     record_parity("reference_" + base + "_f32", base + "_f64", **errs)
