@@ -25,9 +25,12 @@ Default run (one JSON line):
 * ``serving``: a Poisson stream of requests (``--requests``, default 128) served
   with continuous batching: p50/p99 latency, throughput, GPU-busy fraction.
 
-``--impl reference``: rank 0 times the oracle (CPU restatement of the
-reference path, torch CPU with every host thread) on the same workload:
-assembly untimed, then a bounded number of steps.
+``--impl reference``: rank 0 times the reference's own time step on the host
+cores (TorchCor installed under baseline/_ref, torch CPU with every host
+thread; the oracle, its CPU restatement, where it is not installed) on the same
+workload: assembly untimed, then a bounded number of steps.  The default line
+also times the reference's step on the GPU (``reference_gpu``: context, not the
+target).
 """
 from __future__ import annotations
 
@@ -206,23 +209,158 @@ def time_oracle(wl, budget_s, min_steps=2, max_steps=None, warmup=0):
     return dict(value=wl.n_nodes * n / el, steps=n, seconds=el, assemble_s=t_asm, cores=cores, warmup=warmup)
 
 
+REF_DIR = ROOT / "baseline" / "_ref"
+
+
+def import_reference():
+    """The reference package installed under baseline/_ref (``pip install --target``),
+    imported with empty stand-ins for its post-processing imports (pyvista,
+    matplotlib, the ECG module), which the time step never calls; None if absent."""
+    if not (REF_DIR / "torchcor").is_dir():
+        return None
+    import types
+    if str(REF_DIR) not in sys.path:
+        sys.path.insert(0, str(REF_DIR))
+    for name in ["pyvista", "matplotlib", "matplotlib.pyplot", "matplotlib.animation"]:
+        sys.modules.setdefault(name, types.ModuleType(name))
+    ecg = types.ModuleType("torchcor.signalanalysis.signalanalysis.ecg_QS")
+    ecg.Ecg = None
+    sys.modules.setdefault("torchcor.signalanalysis.signalanalysis.ecg_QS", ecg)
+    if not torch.cuda.is_available():
+        torch.cuda.current_device = lambda: 0      # Monodomain.__init__ asks NVML for the GPU
+    import torchcor.core as core
+    import torchcor.ionic as ionic
+    import torchcor.simulator.monodomain as md
+    if not torch.cuda.is_available():
+        class _U:
+            gpu = 0
+            used = 0
+        md.nvmlInit = lambda: None
+        md.nvmlDeviceGetHandleByIndex = lambda i: None
+        md.nvmlDeviceGetUtilizationRates = lambda h: _U()
+        md.nvmlDeviceGetMemoryInfo = lambda h: _U()
+    return md, ionic, core
+
+
+class ReferenceRun:
+    """The reference's own monodomain time step (Monodomain.step with its ionic
+    class, Stimuli, Preconditioner and ConjugateGradient; monodomain.py:109-139) on
+    a workload, on the CPU or a GPU.  The mesh arrays are set as load_mesh sets
+    them (monodomain.py:60-73) and the stimuli are read from .vtx files by the
+    reference; the matrices come from the oracle's restatement of the assembly
+    (bit-identical to Matrices3D.assemble_matrices at every size the tests pin),
+    because the reference assembles through Python lists (minutes at 6 M tets)
+    and assembly is not part of the timed step."""
+
+    def __init__(self, wl, system=None):
+        self.wl = wl
+        self.mods = import_reference()
+        if self.mods is None:
+            raise RuntimeError("reference not installed under baseline/_ref")
+        if system is None:
+            from oracle import port as P
+            osim = oracle_sim(wl)
+            _, _, sm = osim.conductivity.sigma(osim.fibres)
+            t0 = time.perf_counter()
+            system = P.build_system(osim.nodes, osim.elems, sm, wl.dt, torch.float32)
+            self.assemble_s = time.perf_counter() - t0
+        self.system = system
+
+    def build(self, device):
+        md, ionic, core = self.mods
+        wl = self.wl
+        if wl.model == "ttp":
+            im = ionic.TenTusscherPanfilov(wl.cell_type, wl.dt, device=device, dtype=torch.float32)
+        elif wl.model == "crn":
+            im = ionic.CourtemancheRamirezNattel(wl.dt, device=device, dtype=torch.float32)
+        else:
+            im = ionic.ModifiedMS2v(wl.dt, device=device, dtype=torch.float32)
+        sim = md.Monodomain(im, T=wl.T, dt=wl.dt, device=device, dtype=torch.float32)
+        sim.n_nodes = wl.n_nodes
+        sim.nodes = torch.from_numpy(wl.nodes_mm).to(dtype=torch.float32, device=device)
+        sim.elems = torch.from_numpy(np.ascontiguousarray(wl.elems)).to(dtype=torch.int, device=device)
+        sim.regions = torch.from_numpy(np.ascontiguousarray(wl.regions)).to(dtype=torch.int, device=device)
+        sim.fibres = torch.from_numpy(wl.fibres).to(dtype=torch.float32, device=device)
+        sim.stimuli = core.Stimuli(sim.n_nodes, device, torch.float32)
+        sim.conductivity = core.Conductivity(sim.regions, dtype=torch.float32)
+        for c in wl.conductivity:
+            sim.add_conductivity(**c)
+        with tempfile.TemporaryDirectory() as d:
+            for k, st in enumerate(wl.stimuli):
+                f = Path(d) / f"s{k}.vtx"
+                idx = np.asarray(st["region"], dtype=np.int64)
+                f.write_text(f"{len(idx)}\nintra\n" + "\n".join(str(int(i)) for i in idx) + "\n")
+                sim.add_stimulus(str(f), st["start"], st["duration"], st["intensity"], period=wl.T)
+        S = self.system
+        sim.K = S.K.to(device)
+        sim.M = S.M.to(device)
+        A = S.A_coo.to(device)
+        sim.pcd = core.Preconditioner()
+        sim.pcd.create_Jocobi(A)
+        sim.A = A.to_sparse_csr()
+        sim.cg = core.ConjugateGradient(sim.pcd, sim.A, dtype=torch.float64)
+        u = sim.ionic_model.initialize(sim.n_nodes)
+        sim.cg.initialize(x=u, linear_guess=True)
+        return sim, u
+
+    def time(self, device, warmup, budget_s, min_steps=3, max_steps=None, first_step=1):
+        """Steps first_step.. : `warmup` untimed, then until `budget_s` seconds of
+        stepping (at least min_steps, at most max_steps).  Returns node-steps/s etc."""
+        sim, u = self.build(device)
+        wl = self.wl
+        t = 0.0
+        cuda = torch.device(device).type == "cuda"
+        n_done = 0
+        while n_done < first_step - 1 + warmup and n_done < wl.nt - 1:
+            t += wl.dt
+            u, _, _, _ = sim.step(u, t, 1e-5, 1e-5, 100)
+            n_done += 1
+        if cuda:
+            torch.cuda.synchronize(device)
+        n, el, iters = 0, 0.0, 0
+        while (el < budget_s or n < min_steps) and (max_steps is None or n < max_steps) and n_done < wl.nt:
+            t += wl.dt
+            t1 = time.perf_counter()
+            u, it, _, _ = sim.step(u, t, 1e-5, 1e-5, 100)
+            if cuda:
+                torch.cuda.synchronize(device)
+            el += time.perf_counter() - t1
+            n += 1
+            n_done += 1
+            iters += int(it)
+        return dict(value=wl.n_nodes * n / el, steps=n, seconds=el, first=n_done - n + 1,
+                    cg_iterations_per_step=iters / max(n, 1))
+
+
 def reference_arm(a, wl, world, rank):
     if rank != 0:
         return
-    # warm-up steps are run untimed inside the same oracle session; the timed
-    # sample is bounded to keep the whole run within a few minutes
+    # warm-up steps are run untimed inside the same session; the timed sample is
+    # bounded to keep the whole run within a few minutes
     budget = float(os.environ.get("TCB_REFERENCE_BUDGET_S", "60"))
-    r = time_oracle(wl, budget_s=budget, min_steps=min(a.steps, 3), max_steps=a.steps, warmup=a.warmup)
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    if import_reference() is not None:
+        ref = ReferenceRun(wl)
+        r = ref.time("cpu", a.warmup, budget, min_steps=min(a.steps, 3), max_steps=a.steps)
+        kind = "reference"
+        sample = (f"the reference's Monodomain.step (TorchCor 0.1.8 from baseline/_ref, torch CPU, {cores} threads) "
+                  f"on the full workload: {a.warmup} warm-up steps untimed, then {r['steps']} timed steps "
+                  f"({r['seconds']:.1f} s); matrices from the oracle's assembly ({ref.assemble_s:.1f} s, untimed)")
+        r["warmup"] = a.warmup
+    else:
+        r = time_oracle(wl, budget_s=budget, min_steps=min(a.steps, 3), max_steps=a.steps, warmup=a.warmup)
+        kind = "port"
+        sample = (f"oracle (CPU restatement of the reference path, torch CPU, {r['cores']} threads) on the full "
+                  f"workload: assembly {r['assemble_s']:.1f} s and {r['warmup']} warm-up steps untimed, then "
+                  f"{r['steps']} timed steps ({r['seconds']:.1f} s)")
     v = r["value"]
-    sample = (f"oracle (CPU restatement of the reference path, torch CPU, {r['cores']} threads) on the full "
-              f"workload: assembly {r['assemble_s']:.1f} s and {r['warmup']} warm-up steps untimed, then "
-              f"{r['steps']} timed steps ({r['seconds']:.1f} s)")
     line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world, "steps": r["steps"], "warmup": r["warmup"],
             "ms_per_step": 1000 * r["seconds"] / r["steps"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": wl.name, "nodes": wl.n_nodes, "elements": int(len(wl.elems)), "dt_ms": wl.dt,
                        "T_ms": wl.T, "parallelism": "replicas only"},
-            "cpu_baseline": {"value": v, "unit": METRIC, "cores": r["cores"], "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -362,14 +500,40 @@ def tcb_arm(a, wl, world, rank, local, clk):
                "what": f"one Monodomain.solve of the workload (T={wl.T} ms, {wl.nt} steps) from host arrays: "
                        f"mesh upload, assembly, all steps, AT/RT/Vm download and save; wall {wall:.2f} s"}
 
-    cpu = None
+    cpu = ref_gpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         clk.mark(None)
-        r = time_oracle(wl, budget_s=float(os.environ.get("TCB_CPU_BASELINE_S", "15")), min_steps=3, warmup=3)
-        cpu = {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": "port",
-               "sample": f"oracle on the full workload, {r['steps']} steps after an untimed "
-                         f"{r['assemble_s']:.1f} s assembly and {r['warmup']} untimed warm-up steps "
-                         f"({r['seconds']:.1f} s of stepping)"}
+        budget = float(os.environ.get("TCB_CPU_BASELINE_S", "15"))
+        cores = os.cpu_count() or 1
+        torch.set_num_threads(cores)
+        if import_reference() is not None:
+            ref = ReferenceRun(wl)
+            r = ref.time("cpu", 3, budget)
+            cpu = {"value": r["value"], "unit": METRIC, "cores": cores, "kind": "reference",
+                   "sample": f"the reference's Monodomain.step (TorchCor 0.1.8, torch CPU, {cores} threads) on the "
+                             f"full workload: steps {r['first']}..{r['first'] + r['steps'] - 1} timed "
+                             f"({r['seconds']:.1f} s) after 3 untimed; matrices from the oracle's assembly "
+                             f"({ref.assemble_s:.1f} s, untimed)"}
+            if not a.no_reference_gpu:
+                # context, not the target: the reference's own PyTorch step on this GPU
+                clk.mark("reference_gpu")
+                rg = ref.time(dev, 5, 10.0, min_steps=50, max_steps=a.reference_gpu_steps,
+                              first_step=FIRST_TIMED_STEP)
+                clk.mark(None)
+                ref_gpu = {"value": rg["value"], "unit": METRIC, "ms_per_step": 1e3 * rg["seconds"] / rg["steps"],
+                           "steps": [rg["first"], rg["first"] + rg["steps"] - 1],
+                           "cg_iterations_per_step": rg["cg_iterations_per_step"],
+                           "what": "the reference's Monodomain.step (TorchCor 0.1.8: ATen and cuSPARSE kernels, "
+                                   "host-synchronised CG) on this GPU, same workload, wall clock per step with a "
+                                   "synchronize; matrices from the oracle's assembly"}
+                del ref
+                torch.cuda.empty_cache()
+        else:
+            r = time_oracle(wl, budget_s=budget, min_steps=3, warmup=3)
+            cpu = {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": "port",
+                   "sample": f"oracle on the full workload, {r['steps']} steps after an untimed "
+                             f"{r['assemble_s']:.1f} s assembly and {r['warmup']} untimed warm-up steps "
+                             f"({r['seconds']:.1f} s of stepping)"}
     clk.mark(None)
     shape = tuned.get("ionic_shape") or list(_lib.ionic_variants(st.model)[max(tuned["ionic_variant"], 1) - 1])
     return {
@@ -397,6 +561,7 @@ def tcb_arm(a, wl, world, rank, local, clk):
         "full_run": full,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "reference_gpu": ref_gpu,
     }
 
 
@@ -590,6 +755,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-full-run", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own PyTorch step on the GPU")
+    ap.add_argument("--reference-gpu-steps", type=int, default=300)
     ap.add_argument("--no-batch", action="store_true", help="default line without the batch object")
     ap.add_argument("--no-serving", action="store_true", help="default line without the serving object")
     a = ap.parse_args()

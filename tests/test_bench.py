@@ -24,7 +24,9 @@ def test_reference_arm_line():
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["metric"] == "node-steps/s" and line["higher_is_better"]
     assert line["steps"] == 2 and line["warmup"] == 3 and line["value"] > 0
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
+    # the reference itself where it is installed under baseline/_ref, else the oracle
+    kind = "reference" if (ROOT / "baseline" / "_ref" / "torchcor").is_dir() else "port"
+    assert line["cpu_baseline"]["kind"] == kind and line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"] == {"value": line["value"], "unit": "node-steps/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] and line["config"]["nodes"] == 9261
@@ -42,3 +44,29 @@ def test_clock_sampler_counts_marked_segments_only():
     s = c.summary()
     assert s["samples"] == 2 and s["sm_mhz"] == (1965 + 1900) / 2 and s["sm_max_mhz"] == 1965
     assert s["reasons"] == ["sw_power_cap"] and set(s["segments"]) == {"headline", "e2e"}
+
+
+def test_reference_harness_matches_oracle_steps():
+    """The bench's reference harness (the reference's own Monodomain.step with the
+    oracle's matrices) takes the same steps as the oracle, bit for bit."""
+    import pytest
+    import torch
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from torchcor_b200.workloads import ms_cube
+    if bench.import_reference() is None:
+        pytest.skip("reference not installed under baseline/_ref")
+    wl = ms_cube()
+    ref = bench.ReferenceRun(wl)
+    sim, u = ref.build("cpu")
+    osim = bench.oracle_sim(wl)
+    osim.assemble()
+    v = osim.ionic.initialize(osim.n_nodes)
+    osim.cg.initialize(v, linear_guess=True)
+    t = 0.0
+    for _ in range(40):
+        t += wl.dt
+        u, it, _, _ = sim.step(u, t, 1e-5, 1e-5, 100)
+        v, it2 = osim.step(v, t, 1e-5, 1e-5, 100)
+        assert it == it2
+    assert torch.equal(u, v)
