@@ -398,8 +398,10 @@ def tcb_arm(a, wl, world, rank, local, clk):
     # so an ncu capture of them measures the same launches)
     msi, msc = C.c_double(0.0), C.c_double(0.0)
     s0 = sim._sim["next_step"]
+    torch.cuda.nvtx.range_push("profile_window")      # what the ncu captures in profiles/ select
     _lib.check(lib.tcb_mono_profile(C.byref(st), s0, s0 + a.profile_steps, stream.cuda_stream,
                                     C.byref(msi), C.byref(msc)))
+    torch.cuda.nvtx.range_pop()
     sim._sim["next_step"] = s0 + a.profile_steps
     p_iters = sim._sim["step_iters"][s0: s0 + a.profile_steps].sum().item()
     kp = p_iters / a.profile_steps + 1.0

@@ -11,7 +11,8 @@ import pytest
 import torch
 
 from tests.golden import cases as C
-from tests.helpers import case_mesh_dir, device_ionic, golden, oracle_ionic, run_device_tissue, run_oracle_tissue
+from tests.helpers import (case_mesh_dir, device_ionic, golden, oracle_ionic, record_parity, run_device_tissue,
+                           run_oracle_tissue)
 
 pytestmark = pytest.mark.gpu
 
@@ -191,8 +192,11 @@ def test_error_against_float64_reference(lib, cuda, name, ref64, tmp_path):
     Vm = torch.load(out / "Vm.pt").numpy()
     if "Vm_idx" in g:
         Vm = Vm[g["Vm_idx"]]
-    assert np.abs(AT - g["AT"]).max() <= case["dt"] * 1.001
-    assert np.abs(Vm - g["Vm"]).max() / np.abs(g["Vm"]).max() <= 1e-3
+    at_err = np.abs(AT - g["AT"]).max()
+    vm_err = np.abs(Vm - g["Vm"]).max() / np.abs(g["Vm"]).max()
+    record_parity(name, ref64, at_max=at_err, at_max_steps=int(round(at_err / case["dt"])), vm_rel=vm_err)
+    assert at_err <= case["dt"] * 1.001
+    assert vm_err <= 1e-3
 
 
 def test_step_api_matches_oracle(lib, cuda, tmp_path):
