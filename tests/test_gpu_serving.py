@@ -25,3 +25,30 @@ def test_served_requests_match_alone(lib, cuda):
         vm = alone.current_solution().cpu().numpy()
         assert np.abs(r.result["Vm"].numpy() - vm).max() <= 1e-3 * np.abs(vm).max()
         assert abs(r.n_total_iter - alone.n_total_iter) <= max(3, alone.n_total_iter // 50)
+
+
+@pytest.mark.parametrize("mesh,size", [("cube", 79), ("ico", 8)])
+@pytest.mark.parametrize("model", ["ms", "ttp", "crn"])
+def test_admission_estimate_covers_device_memory(lib, cuda, mesh, size, model):
+    """The server admits requests by serving.footprint_bytes; a request of the large
+    end of the mix (512,000-node cube, 655,362-node icosphere) must not hold more
+    device memory than that estimate once built and added to a batch."""
+    import torch
+    from torchcor_b200 import serving
+    from torchcor_b200.simulator import MonodomainBatch
+    req = serving.Request(0, 0.0, mesh, size, model, 50.0)
+    batch = MonodomainBatch(cuda)
+    torch.cuda.synchronize(cuda)
+    base = torch.cuda.memory_allocated(cuda)
+    torch.cuda.reset_peak_memory_stats(cuda)
+    sim = serving.build_sim(req, cuda)
+    sim.prepare(req.a_tol, req.r_tol, req.max_iter, snapshot_interval=req.T)
+    batch.add(sim, req.a_tol, req.r_tol, req.max_iter, snapshot_interval=req.T)
+    batch.step(1)
+    torch.cuda.synchronize(cuda)
+    held = torch.cuda.memory_allocated(cuda) - base
+    peak = torch.cuda.max_memory_allocated(cuda) - base
+    est = serving.footprint_bytes(req)
+    print(f"{mesh}{size} {model}: nodes {req.n_nodes}, held {held / 2**20:.0f} MiB, "
+          f"build peak {peak / 2**20:.0f} MiB, estimate {est / 2**20:.0f} MiB")
+    assert held <= est, (held, est)
