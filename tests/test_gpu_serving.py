@@ -33,11 +33,14 @@ def test_admission_estimate_covers_device_memory(lib, cuda, mesh, size, model):
     """The server admits requests by serving.footprint_bytes; a request of the large
     end of the mix (512,000-node cube, 655,362-node icosphere) must not hold more
     device memory than that estimate once built and added to a batch."""
+    import gc
+
     import torch
     from torchcor_b200 import serving
     from torchcor_b200.simulator import MonodomainBatch
     req = serving.Request(0, 0.0, mesh, size, model, 50.0)
     batch = MonodomainBatch(cuda)
+    gc.collect()                       # earlier tests' tensors are released before the baseline
     torch.cuda.synchronize(cuda)
     base = torch.cuda.memory_allocated(cuda)
     torch.cuda.reset_peak_memory_stats(cuda)

@@ -141,11 +141,24 @@ _STATES = {"ms": 1, "ttp": 19, "crn": 19}
 
 
 def footprint_bytes(req: Request) -> int:
-    """Conservative device bytes of a request while it runs: CSR and sliced-ELL
-    matrices (~40 B per stored non-zero), 16 vectors, the ionic state and tables."""
+    """Device bytes a request holds while it runs, with a 10 % margin: the CSR copy
+    (int32 columns, float32 M, K/chi, A, K' - 20 B per non-zero) and the sliced-ELL
+    solver copy (int32 and int16 columns, float32 M, K', A - 18 B per stored entry,
+    slices padded to their widest row), 13 per-node vectors (solution ring, CG
+    vectors, 1/diag, AT/RT, stimulus bits) and the ionic state, the mesh arrays the
+    simulation keeps (coordinates, elements, regions, fibres), the per-step
+    schedule and the lookup tables.  Checked against the memory a built request
+    holds by the GPU tests."""
     n = req.n_nodes
-    nnz_row = 15 if req.mesh == "cube" else 7
-    return int(n * (nnz_row * 40 + 16 * 4 + 4 * _STATES[req.model]) + 8 * (req.nt + 1) + _TABLE_BYTES[req.model])
+    if req.mesh == "cube":
+        n_elems, k, nnz_row = 6 * req.size ** 3, 4, 15
+    else:
+        n_elems, k, nnz_row = 20 * 4 ** req.size, 3, 7
+    nnz = n * nnz_row
+    matrices = 20 * nnz + 4 * (n + 1) + 18 * nnz * 1.1
+    vectors = n * (13 * 4 + 4 * _STATES[req.model])
+    mesh = 12 * n + (4 * k + 16) * n_elems
+    return int(1.1 * (matrices + vectors + mesh) + 12 * (req.nt + 1) + _TABLE_BYTES[req.model])
 
 
 class Server:
