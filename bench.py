@@ -550,7 +550,9 @@ def tcb_arm(a, wl, world, rank, local, clk):
                    "simulated_ms_per_s": world * wl.dt * a.steps / (ms / 1e3),
                    "tuned": {"ionic_variant": int(tuned["ionic_variant"]),
                              "ionic_nodes_per_thread": int(shape[0]), "ionic_blocks_per_sm": int(shape[1]),
-                             "ionic_fast_math": int(shape[2]), "cg_blocks_per_sm": int(tuned["cg_per_sm"]),
+                             "ionic_fast_math": int(shape[2]),
+                             "ionic_staged": int(shape[3]) if len(shape) > 3 else 0,
+                             "cg_blocks_per_sm": int(tuned["cg_per_sm"]),
                              "fused_step": int(tuned.get("fused_step", 0)),
                              "source": "cache" if tuned.get("cached") else "measured"}},
         "gpu_launches": (1 if fused else 2) * a.steps,

@@ -144,10 +144,11 @@ int tcb_model_table_info(int32_t model, int32_t index, int64_t* rows, int32_t* n
  * instances; instance `variant` (1..count, 0 = the default) handles *nodes_per_thread consecutive
  * nodes per thread (structure-of-arrays state moved as 4-, 8- or 16-byte vectors) with the register
  * budget of *blocks_per_sm 256-thread blocks per SM; *fast_math = 1 if it divides and takes
- * logarithms with the hardware approximations (a few ulp), 0 for IEEE division and logf.
- * TCB_ERANGE past the last instance. */
+ * logarithms with the hardware approximations (a few ulp), 0 for IEEE division and logf;
+ * *staged = 1 for the persistent form that bulk-copies the next tile of nodes into shared memory
+ * while it computes the current one.  TCB_ERANGE past the last instance. */
 int tcb_ionic_variant(int32_t model, int32_t variant, int32_t* count, int32_t* nodes_per_thread,
-                      int32_t* blocks_per_sm, int32_t* fast_math);
+                      int32_t* blocks_per_sm, int32_t* fast_math, int32_t* staged);
 /* construct_tables (TTP :197-318, CRN :212-328); no-op for MS.  `tables` must be
  * 16-byte aligned (TCB_EINVAL otherwise), as in every call that reads it. */
 int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream);

@@ -40,9 +40,9 @@ def test_ionic_variant_table(lib):
     for model in (_lib.MODEL_MS, _lib.MODEL_TTP, _lib.MODEL_CRN):
         shapes = _lib.ionic_variants(model)
         assert len(shapes) >= 3
-        assert all(v in (1, 2, 4) and b >= 1 and f in (0, 1) for v, b, f in shapes)
-        assert any(v == 1 for v, _, _ in shapes)          # the fallback for unaligned arrays
-    cnt, v, b, f = (C.c_int32() for _ in range(4))
-    assert lib.tcb_ionic_variant(_lib.MODEL_TTP, 99, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f)) == \
-        _lib.TCB_ERANGE
-    assert lib.tcb_ionic_variant(7, 0, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f)) == _lib.TCB_EINVAL
+        assert all(v in (1, 2, 4) and b >= 1 and f in (0, 1) and st in (0, 1) for v, b, f, st in shapes)
+        assert any(v == 1 and st == 0 for v, _, _, st in shapes)   # the fallback for unaligned arrays
+    cnt, v, b, f, st = (C.c_int32() for _ in range(5))
+    args = (C.byref(cnt), C.byref(v), C.byref(b), C.byref(f), C.byref(st))
+    assert lib.tcb_ionic_variant(_lib.MODEL_TTP, 99, *args) == _lib.TCB_ERANGE
+    assert lib.tcb_ionic_variant(7, 0, *args) == _lib.TCB_EINVAL

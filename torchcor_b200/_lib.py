@@ -87,7 +87,7 @@ SIGNATURES = [
     ("tcb_model_layout", C.c_int, [_i32, _vp, _pi64, _pi64]),
     ("tcb_model_table_info", C.c_int, [_i32, _i32, _pi64, C.POINTER(_i32), C.POINTER(_i32), _pi64]),
     ("tcb_ionic_variant", C.c_int, [_i32, _i32, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32),
-                                    C.POINTER(_i32)]),
+                                    C.POINTER(_i32), C.POINTER(_i32)]),
     ("tcb_model_tables", C.c_int, [_i32, _vp, _vp, _vp]),
     ("tcb_model_init", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp]),
     ("tcb_model_differentiate", C.c_int, [_i32, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp]),
@@ -183,13 +183,13 @@ def model_states(model):
 
 
 def ionic_variants(model):
-    """[(nodes_per_thread, blocks_per_sm, fast_math)] of the model's ionic kernel
-    instances (instance k + 1 in ``tcb_mono.ionic_variant``); entry 0 is the default."""
+    """[(nodes_per_thread, blocks_per_sm, fast_math, staged)] of the model's ionic
+    kernel instances (instance k + 1 in ``tcb_mono.ionic_variant``); entry 0 is the default."""
     lib = load()
-    cnt, v, b, f = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
-    check(lib.tcb_ionic_variant(model, 0, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f)))
+    cnt, v, b, f, st = (C.c_int32() for _ in range(5))
+    check(lib.tcb_ionic_variant(model, 0, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f), C.byref(st)))
     out = []
     for k in range(1, cnt.value + 1):
-        check(lib.tcb_ionic_variant(model, k, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f)))
-        out.append((v.value, b.value, f.value))
+        check(lib.tcb_ionic_variant(model, k, C.byref(cnt), C.byref(v), C.byref(b), C.byref(f), C.byref(st)))
+        out.append((v.value, b.value, f.value, st.value))
     return out

@@ -31,6 +31,7 @@
 
 #include "l2_hint.cuh"
 #include "batch.cuh"
+#include "bulk.cuh"
 #include "cg_common.cuh"
 #include "tcb_internal.h"
 
@@ -210,35 +211,6 @@ __device__ __forceinline__ void ap_slice(const CgView& d, const float* pin, floa
 // ELL array its entries are one contiguous block (column-major slices).
 constexpr int kStages = 2;             // units in flight per warp
 constexpr int kMaxUnitEntries = 16;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// global -> shared bulk copy (no multicast); 16-byte aligned addresses, size a multiple of 16
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
 
 // warp-uniform wait for a stage's copies; gives up after the timeout (error
 // word set) so a lost copy can never hang the kernel
@@ -498,7 +470,7 @@ __device__ __forceinline__ void issue(Pipe& P, int s, const CgView& d, const Wal
     if (lane == 0) {
         const int nk = u.count();
         // order this warp's earlier shared-memory reads of the stage before the async writes
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        fence_proxy_async_smem();
         mbar_arrive_tx(P.bar + s, (uint32_t)(nk * TCB_SLICE * Streams::entry_bytes(d)));
         if (!P.drop)
             Streams::copy(d, u.s0 + (int64_t)u.k0 * TCB_SLICE, nk, P.buf + (size_t)s * P.stage_bytes, P.bar + s);
@@ -771,7 +743,7 @@ __global__ void __launch_bounds__(kCgThreads, PER_SM) batch_cg_kernel(const Batc
         P.drop = (W->wait.drop_first_copy && blockIdx.x == 0 && warp == 0) ? 1u : 0u;
         if (lane == 0) {
             for (int st = 0; st < kStages; ++st) mbar_init(P.bar + st);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            mbar_init_fence();
         }
         __syncwarp();
     }
