@@ -238,24 +238,25 @@ struct Shapes<MS> {
 };
 template <>
 struct Shapes<TTP> {
-    static constexpr int kCount = 10;
-    static constexpr Shape shape[kCount] = {{1, 4, 0, 0}, {1, 6, 0, 0}, {2, 3, 0, 0}, {4, 2, 0, 0}, {1, 2, 1, 0},
-                                            {1, 3, 1, 0}, {2, 2, 1, 0}, {4, 1, 1, 0}, {2, 2, 1, 1}, {2, 2, 0, 1}};
+    static constexpr int kCount = 11;
+    static constexpr Shape shape[kCount] = {{1, 4, 0, 0}, {1, 6, 0, 0}, {2, 3, 0, 0}, {4, 2, 0, 0},
+                                            {1, 2, 1, 0}, {1, 3, 1, 0}, {2, 2, 1, 0}, {4, 1, 1, 0},
+                                            {2, 2, 1, 1}, {1, 3, 1, 1}, {1, 4, 1, 1}};
     static constexpr LaunchFn<TTP> fn[kCount] = {
         launch_shape<TTP, 1, 4, QExact>, launch_shape<TTP, 1, 6, QExact>,  launch_shape<TTP, 2, 3, QExact>,
         launch_shape<TTP, 4, 2, QExact>, launch_shape<TTP, 1, 2, QFast>,   launch_shape<TTP, 1, 3, QFast>,
         launch_shape<TTP, 2, 2, QFast>,  launch_shape<TTP, 4, 1, QFast>,   launch_staged<TTP, 2, 2, QFast>,
-        launch_staged<TTP, 2, 2, QExact>};
+        launch_staged<TTP, 1, 3, QFast>, launch_staged<TTP, 1, 4, QFast>};
 };
 template <>
 struct Shapes<CRN> {
-    static constexpr int kCount = 7;
-    static constexpr Shape shape[kCount] = {{2, 2, 1, 0}, {1, 3, 1, 0}, {1, 2, 1, 0}, {4, 1, 1, 0},
-                                            {1, 3, 0, 0}, {2, 2, 0, 0}, {2, 2, 1, 1}};
+    static constexpr int kCount = 9;
+    static constexpr Shape shape[kCount] = {{2, 2, 1, 0}, {1, 3, 1, 0}, {1, 2, 1, 0}, {4, 1, 1, 0}, {1, 3, 0, 0},
+                                            {2, 2, 0, 0}, {2, 2, 1, 1}, {1, 3, 1, 1}, {1, 4, 1, 1}};
     static constexpr LaunchFn<CRN> fn[kCount] = {
         launch_shape<CRN, 2, 2, QFast>,  launch_shape<CRN, 1, 3, QFast>,  launch_shape<CRN, 1, 2, QFast>,
         launch_shape<CRN, 4, 1, QFast>,  launch_shape<CRN, 1, 3, QExact>, launch_shape<CRN, 2, 2, QExact>,
-        launch_staged<CRN, 2, 2, QFast>};
+        launch_staged<CRN, 2, 2, QFast>, launch_staged<CRN, 1, 3, QFast>, launch_staged<CRN, 1, 4, QFast>};
 };
 
 inline bool aligned(const void* p, unsigned bytes) { return ((uintptr_t)p & (bytes - 1)) == 0; }

@@ -96,9 +96,10 @@ __device__ __forceinline__ void ld_nodes(const T* __restrict__ p, T (&o)[V]) {
 
 template <int V>
 __device__ __forceinline__ void st_nodes(float* __restrict__ p, const float (&v)[V]) {
-    static_assert(V == 2 || V == 4, "2 or 4 floats");
+    static_assert(V == 1 || V == 2 || V == 4, "1, 2 or 4 floats");
     if constexpr (V == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-    else *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    else if constexpr (V == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    else *p = v[0];
 }
 
 // ionic_node for the V consecutive nodes i0 .. i0+V-1 (V = 1, 2 or 4; Q the
