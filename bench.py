@@ -608,6 +608,7 @@ def batch_arm(a, world, rank, local, clk, steps=None):
     if world > 1:
         torch.distributed.barrier()
     clk.mark("batch")
+    torch.cuda.nvtx.range_push("batch_timed")         # what the ncu captures in profiles/ select
     e0.record(stream)
     done = 0
     if replay:
@@ -617,6 +618,7 @@ def batch_arm(a, world, rank, local, clk, steps=None):
     if K > done:
         batch.step(K - done)
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize(dev)
     clk.mark(None)
     ms = replicas.reduce_max(e0.elapsed_time(e1))     # slowest rank (each rank runs the batch)
