@@ -154,9 +154,15 @@ int tcb_ionic_variant(int32_t model, int32_t variant, int32_t* count, int32_t* n
 int tcb_model_tables(int32_t model, const double* params, float* tables, void* stream);
 /* initialize(n_nodes): fill state rows and V with the initial values */
 int tcb_model_init(int32_t model, const double* params, float* state, int64_t n_pad, float* v, void* stream);
-/* differentiate(V): dv = -Iion and the state update, for n nodes (`tables` 16-byte aligned) */
-int tcb_model_differentiate(int32_t model, const double* params, const float* tables, float* state,
-                            int64_t n_pad, int64_t n, const float* v, float* dv, void* stream);
+/* Per-node parameters of `model` (comma-separated names, "" if none): TTP "GCaL,GKr,GKs,Gto" — the
+ * reference's per-node conductance tensors (TenTusscherPanfilov.py:327-330), which initialize() fills
+ * uniformly and a caller may overwrite node by node.  A node_params array holds them as rows of
+ * n_pad floats in this order; NULL means the uniform values of the *_init parameters. */
+const char* tcb_model_node_params(int32_t model);
+/* differentiate(V): dv = -Iion and the state update, for n nodes (`tables` 16-byte aligned;
+ * node_params as above, or NULL) */
+int tcb_model_differentiate(int32_t model, const double* params, const float* tables, const float* node_params,
+                            float* state, int64_t n_pad, int64_t n, const float* v, float* dv, void* stream);
 
 /* ---------------------------------------------------------------- time loop
  * One simulation on the device.  Replaces Monodomain.step / solve's loop
@@ -219,6 +225,8 @@ typedef struct tcb_mono {
     uint32_t* barrier;       /* [4] grid-barrier words */
     /* model parameters (host) */
     const double* params;
+    /* per-node model parameters (tcb_model_node_params), n_pad floats per row, or NULL */
+    const float* node_params;
 } tcb_mono;
 
 int64_t tcb_mono_scratch_doubles(void);

@@ -57,6 +57,12 @@ CASES = [
     dict(kind="tissue", name="cube4_ms_rt_f32", model="ms", dtype="f32",
          mesh=dict(type="cube", n=4, h=0.5, fibres="x", regions="one"), conductivity=_ONE, stimuli=_FACE,
          dt=0.02, T=450.0, tol=1e-5, max_iter=100, snapshots=[0, 1, 2, 100, 200, 400, 450], keep_states=True),
+    # per-node TTP conductances set after initialize() and stepped through Monodomain.step
+    # (the reference's solve() re-initialises them to uniform values)
+    dict(kind="step_api", name="cube8_ttp_nodecond_f32", model="ttp", cell_type="ENDO", dtype="f32",
+         mesh=dict(type="cube", n=8, h=0.25, fibres="rotz", regions="splitx"), conductivity=_TTP_COND,
+         stimuli=_TTP_STIM, dt=0.01, T=30.0, tol=1e-5, max_iter=100, every=100,
+         node_cond=dict(GKs=(0.1, 0.4), Gto=(0.3, 0.05), GKr=(0.1, 0.2), GCaL=(3e-5, 5e-5))),
     # one differentiate() on seeded random inputs spanning the lookup-table ranges
     dict(_STEP, name="step_ms_f32", model="ms", dtype="f32"),
     dict(_STEP, name="step_ttp_f32", model="ttp", cell_type="ENDO", dtype="f32"),
@@ -182,3 +188,8 @@ def random_ionic_inputs(case):
             st[g] = rng.uniform(0.0, 1.0, size=n)
     dt = np.float64 if case["dtype"] == "f64" else np.float32
     return V.astype(dt), {k: v.astype(dt) for k, v in st.items()}
+
+
+def node_values(lo, hi, n):
+    """Per-node parameter values rising linearly with the node index (float32)."""
+    return (lo + (hi - lo) * np.arange(n, dtype=np.float64) / max(n - 1, 1)).astype(np.float32)

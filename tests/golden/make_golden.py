@@ -202,6 +202,41 @@ def states_of(im, model):
     return {n: getattr(im, n).clone().numpy() for n in names}
 
 
+def run_step_api(md, ionic, case, workdir):
+    """Monodomain.step driven step by step (monodomain.py:109-139), as a caller of
+    the reference does to change per-node model parameters after initialize():
+    assemble, initialize, set the per-node values, then step with the reference's
+    own time accumulation; Vm every ``every`` steps and the iteration counts."""
+    dtype = torch.float64 if case["dtype"] == "f64" else torch.float32
+    mesh_dir = Path(workdir) / case["name"]
+    C.write_case_mesh(case, mesh_dir)
+    im = make_ionic(ionic, case["model"], case["dt"], dtype, case)
+    sim = md.Monodomain(im, T=case["T"], dt=case["dt"], device=torch.device("cpu"), dtype=dtype)
+    sim.load_mesh(mesh_dir)
+    for cond in case["conductivity"]:
+        sim.add_conductivity(**cond)
+    for s in case["stimuli"]:
+        sim.add_stimulus(str(mesh_dir / s["file"]), start=s["start"], duration=s["duration"],
+                         intensity=s["intensity"], period=s.get("period"), count=s.get("count", 1))
+    sim.assemble()
+    u = sim.ionic_model.initialize(sim.n_nodes)
+    for name, (lo, hi) in case["node_cond"].items():
+        setattr(im, name, torch.from_numpy(C.node_values(lo, hi, sim.n_nodes)).to(dtype))
+    sim.cg.initialize(x=u, linear_guess=True)
+    t = 0.0
+    frames, iters = [u.clone()], []
+    for k in range(1, int(case["T"] / case["dt"]) + 1):
+        t += case["dt"]
+        u, it, _, _ = sim.step(u, t, case["tol"], case["tol"], case["max_iter"])
+        iters.append(it)
+        if k % case["every"] == 0:
+            frames.append(u.clone())
+    fx = dict(Vm=torch.stack(frames).numpy(), iters=np.asarray(iters, dtype=np.int16))
+    for k, v in states_of(im, case["model"]).items():
+        fx["state_" + k] = v
+    return fx
+
+
 def run_single_step(ionic, case):
     """One ``differentiate`` on seeded random inputs across the V range."""
     dtype = torch.float64 if case["dtype"] == "f64" else torch.float32
@@ -263,6 +298,8 @@ def main():
             kind = case["kind"]
             if kind == "tissue":
                 fx = run_tissue(md, ionic, case, work)
+            elif kind == "step_api":
+                fx = run_step_api(md, ionic, case, work)
             elif kind == "step":
                 fx = run_single_step(ionic, case)
             else:

@@ -282,7 +282,7 @@ def test_misaligned_tables_rejected_before_any_launch(lib):
     model = _lib.MODEL_TTP
     params = np.zeros(len(_lib.model_params(model)), dtype=np.float64)
     fake = 1 << 20
-    st = lib.tcb_model_differentiate(model, _lib.ptr(params), fake + 4, fake, 1, 1, fake, fake, None)
+    st = lib.tcb_model_differentiate(model, _lib.ptr(params), fake + 4, None, fake, 1, 1, fake, fake, None)
     assert st == _lib.TCB_EINVAL
     assert lib.tcb_model_tables(model, _lib.ptr(params), fake + 8, None) == _lib.TCB_EINVAL
 

@@ -236,3 +236,41 @@ def test_state_attributes_are_views(lib, cuda):
     assert m.Cai.shape == (100,) and float(m.Cai[3]) == pytest.approx(0.00007)
     m.Cai = torch.full((100,), 1e-4)
     assert float(m.Cai[7]) == pytest.approx(1e-4)
+
+
+def test_per_node_conductances_through_step(lib, cuda, tmp_path):
+    """TTP conductances (GCaL, GKr, GKs, Gto) set node by node after initialize() and
+    stepped through Monodomain.step, as a reference caller does
+    (TenTusscherPanfilov.py:327-330, monodomain.py:109-139): Vm within 1e-3 of the
+    reference's range at every stored frame, CG iterations within 2 %."""
+    from torchcor_b200.simulator import Monodomain
+    case = C.case("cube8_ttp_nodecond_f32")
+    g = golden(case["name"])
+    d = case_mesh_dir(case, tmp_path)
+    im = device_ionic(case, cuda)
+    sim = Monodomain(im, T=case["T"], dt=case["dt"], device=cuda)
+    sim.load_mesh(d)
+    for c in case["conductivity"]:
+        sim.add_conductivity(**c)
+    for s in case["stimuli"]:
+        sim.add_stimulus(str(d / s["file"]), s["start"], s["duration"], s["intensity"])
+    sim.assemble()
+    sim._setup(case["tol"], case["tol"], case["max_iter"], True, True, 1, False)
+    assert im.node_params is None and float(im.GKs[0]) == pytest.approx(0.392)   # uniform after initialize
+    for name, (lo, hi) in case["node_cond"].items():
+        setattr(im, name, torch.from_numpy(C.node_values(lo, hi, sim.n_nodes)))
+    assert im.node_params is not None and float(im.GKs[-1]) == pytest.approx(0.4)
+    u = sim.current_solution().clone()
+    t, frames, iters = 0.0, [u.cpu().numpy()], []
+    for k in range(1, int(case["T"] / case["dt"]) + 1):
+        t += case["dt"]
+        u, it, _, _ = sim.step(u, t, case["tol"], case["tol"], case["max_iter"])
+        iters.append(it)
+        if k % case["every"] == 0:
+            frames.append(u.cpu().numpy())
+    vm = np.stack(frames)
+    assert np.abs(vm - g["Vm"]).max() <= 1e-3 * np.abs(g["Vm"]).max()
+    assert abs(sum(iters) - int(g["iters"].sum())) <= max(3, int(g["iters"].sum()) // 50)
+    # the per-node values reached the kernels: the same case with uniform conductances differs
+    ref_uniform = golden("cube8_ttp_f32")["Vm"][:31]
+    assert np.abs(ref_uniform - g["Vm"]).max() > 100 * np.abs(vm - g["Vm"]).max()

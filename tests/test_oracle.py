@@ -104,3 +104,33 @@ def test_reference_float32_vs_float64_spread(base):
     errs["iters_total"], errs["iters_total_ref"] = int(a["n_total_iter"]), int(b["n_total_iter"])
     record_parity("reference_" + base + "_f32", base + "_f64", **errs)
     assert errs["at_max_steps"] <= 1 and errs["vm_rel_outside_upstroke"] <= 1e-3
+
+
+def test_oracle_per_node_conductances_step_api(tmp_path):
+    """The oracle through Monodomain.step with TTP conductances set node by node after
+    initialize() reproduces the reference's fixture bit for bit."""
+    from oracle import port as P
+    case = C.case("cube8_ttp_nodecond_f32")
+    g = golden(case["name"])
+    d = case_mesh_dir(case, tmp_path)
+    sim = P.Monodomain(oracle_ionic(case), case["T"], case["dt"], torch.float32)
+    sim.load_mesh(d)
+    for c in case["conductivity"]:
+        sim.add_conductivity(**c)
+    for s in case["stimuli"]:
+        sim.add_stimulus(str(d / s["file"]), s["start"], s["duration"], s["intensity"], s.get("period"),
+                         s.get("count", 1))
+    sim.assemble()
+    u = sim.ionic.initialize(sim.n_nodes)
+    for name, (lo, hi) in case["node_cond"].items():
+        setattr(sim.ionic, name, torch.from_numpy(C.node_values(lo, hi, sim.n_nodes)))
+    sim.cg.initialize(u, linear_guess=True)
+    t, frames, iters = 0.0, [u.clone()], []
+    for k in range(1, int(case["T"] / case["dt"]) + 1):
+        t += case["dt"]
+        u, it = sim.step(u, t, case["tol"], case["tol"], case["max_iter"])
+        iters.append(it)
+        if k % case["every"] == 0:
+            frames.append(u.clone())
+    assert np.array_equal(np.asarray(iters), g["iters"])
+    assert np.array_equal(torch.stack(frames).numpy(), g["Vm"])

@@ -48,6 +48,7 @@ class tcb_mono(C.Structure):
         ("fused_step", _i32),
         ("step_iters", _vp), ("counter", _vp), ("scratch", _vp), ("barrier", _vp),
         ("params", _vp),
+        ("node_params", _vp),
     ]
 
 
@@ -90,7 +91,8 @@ SIGNATURES = [
                                     C.POINTER(_i32), C.POINTER(_i32)]),
     ("tcb_model_tables", C.c_int, [_i32, _vp, _vp, _vp]),
     ("tcb_model_init", C.c_int, [_i32, _vp, _vp, _i64, _vp, _vp]),
-    ("tcb_model_differentiate", C.c_int, [_i32, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp]),
+    ("tcb_model_node_params", C.c_char_p, [_i32]),
+    ("tcb_model_differentiate", C.c_int, [_i32, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp]),
     ("tcb_mono_scratch_doubles", _i64, []),
     ("tcb_mono_run", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),
     ("tcb_mono_cg_run", C.c_int, [C.POINTER(tcb_mono), _i64, _i64, _vp]),
@@ -180,6 +182,12 @@ def table_layout(model):
 
 def model_states(model):
     return load().tcb_model_states(model).decode().split(",")
+
+
+def model_node_params(model):
+    """Names of the model's per-node parameters (rows of tcb_mono.node_params)."""
+    s = load().tcb_model_node_params(model).decode()
+    return s.split(",") if s else []
 
 
 def ionic_variants(model):

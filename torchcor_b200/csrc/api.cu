@@ -55,6 +55,7 @@ MonoDev make_dev(const tcb_mono* m) {
     d.snap_ring = m->snap_ring;
     d.cg_per_sm = m->cg_per_sm;
     d.stim_bits = m->stim_bits;
+    d.node_params = m->node_params;
     d.step_t = m->step_t;
     d.step_stim = m->step_stim;
     d.step_iters = m->step_iters;

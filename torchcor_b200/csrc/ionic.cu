@@ -38,13 +38,13 @@ inline unsigned grid_for(int64_t n) {
 }
 
 template <class M>
-__global__ void differentiate_kernel(typename M::C c, typename M::Tables T, float* state, int64_t n_pad, int64_t n,
-                                     const float* __restrict__ v, float* __restrict__ dv) {
+__global__ void differentiate_kernel(typename M::C c, typename M::Tables T, const float* node_params, float* state,
+                                     int64_t n_pad, int64_t n, const float* __restrict__ v, float* __restrict__ dv) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         float s[M::kStates];
 #pragma unroll
         for (int k = 0; k < M::kStates; ++k) s[k] = state[k * n_pad + i];
-        float d = M::template step<QFast>(v[i], s, c, T);
+        float d = M::template step<QFast>(v[i], s, c, T, M::node_g(c, node_params, n_pad, i));
 #pragma unroll
         for (int k = 0; k < M::kStates; ++k) state[k * n_pad + i] = s[k];
         dv[i] = d;
@@ -171,7 +171,10 @@ __global__ void __launch_bounds__(kThreads, MINB) mono_ionic_staged_kernel(MonoD
                 for (int j = 0; j < V; ++j) s[j][q] = buf[q * kTile + j0 + j];
             float b[V];
 #pragma unroll
-            for (int j = 0; j < V; ++j) b[j] = v[j] * d.cm + d.dt * Q::div(M::template step<Q>(v[j], s[j], c, T), 100.0f);
+            for (int j = 0; j < V; ++j)
+                b[j] = v[j] * d.cm +
+                       d.dt * Q::div(M::template step<Q>(v[j], s[j], c, T, M::node_g(c, d.node_params, d.n_pad, i0 + j)),
+                                     100.0f);
 #pragma unroll
             for (int q = 0; q < S; ++q) {
                 float t[V];
@@ -282,10 +285,10 @@ int launch_mono(const tcb_mono* m, const MonoDev& d, cudaStream_t s) {
 }
 
 template <class M>
-int run_differentiate(const double* params, const float* tables, float* state, int64_t n_pad, int64_t n,
-                      const float* v, float* dv, cudaStream_t s) {
-    differentiate_kernel<M><<<grid_for(n), kThreads, 0, s>>>(M::derive(params), M::tables(tables, params), state,
-                                                             n_pad, n, v, dv);
+int run_differentiate(const double* params, const float* tables, const float* node_params, float* state,
+                      int64_t n_pad, int64_t n, const float* v, float* dv, cudaStream_t s) {
+    differentiate_kernel<M><<<grid_for(n), kThreads, 0, s>>>(M::derive(params), M::tables(tables, params),
+                                                             node_params, state, n_pad, n, v, dv);
     TCB_CHECK_LAUNCH("differentiate kernel");
     return TCB_OK;
 }
@@ -324,19 +327,29 @@ int launch_mono_finish(const MonoDev& d, cudaStream_t s) {
 
 using namespace tcb;
 
-extern "C" int tcb_model_differentiate(int32_t model, const double* params, const float* tables, float* state,
-                                       int64_t n_pad, int64_t n, const float* v, float* dv, void* stream) {
+extern "C" int tcb_model_differentiate(int32_t model, const double* params, const float* tables,
+                                       const float* node_params, float* state, int64_t n_pad, int64_t n,
+                                       const float* v, float* dv, void* stream) {
     if (!params || !state || !v || !dv || n <= 0 || n_pad < n) return fail(TCB_EINVAL, "tcb_model_differentiate: bad arguments");
     if (model != TCB_MODEL_MS && !tables) return fail(TCB_EINVAL, "tcb_model_differentiate: null tables");
     if (model != TCB_MODEL_MS && ((uintptr_t)tables & 15u))
         return fail(TCB_EINVAL, "tcb_model_differentiate: tables not 16-byte aligned");
     cudaStream_t s = as_stream(stream);
     switch (model) {
-        case TCB_MODEL_MS: return run_differentiate<MS>(params, tables, state, n_pad, n, v, dv, s);
-        case TCB_MODEL_TTP: return run_differentiate<TTP>(params, tables, state, n_pad, n, v, dv, s);
-        case TCB_MODEL_CRN: return run_differentiate<CRN>(params, tables, state, n_pad, n, v, dv, s);
+        case TCB_MODEL_MS: return run_differentiate<MS>(params, tables, node_params, state, n_pad, n, v, dv, s);
+        case TCB_MODEL_TTP: return run_differentiate<TTP>(params, tables, node_params, state, n_pad, n, v, dv, s);
+        case TCB_MODEL_CRN: return run_differentiate<CRN>(params, tables, node_params, state, n_pad, n, v, dv, s);
     }
     return fail(TCB_EINVAL, "unknown ionic model");
+}
+
+extern "C" const char* tcb_model_node_params(int32_t model) {
+    switch (model) {
+        case TCB_MODEL_MS: return "";
+        case TCB_MODEL_TTP: return "GCaL,GKr,GKs,Gto";
+        case TCB_MODEL_CRN: return "";
+    }
+    return nullptr;
 }
 
 extern "C" int tcb_ionic_variant(int32_t model, int32_t variant, int32_t* count, int32_t* nodes_per_thread,

@@ -140,6 +140,11 @@ struct CRN {
         return c;
     }
 
+    // no per-node parameters
+    static constexpr int kNodeParams = 0;
+    struct NodeG {};
+    __host__ __device__ static NodeG node_g(const C&, const float*, int64_t, int64_t) { return NodeG{}; }
+
     static int64_t table_floats(const double*) {
         return kV.floats() + kCai.floats() + kFn.floats();
     }
@@ -268,7 +273,7 @@ struct CRN {
     // The reference's order of operations; division and logarithm from the
     // policy Q (QFast or QExact, ionic_common.cuh).
     template <class Q>
-    __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
+    __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T, const NodeG&) {
         LutPos pv = lut_pos<Q>(V, T.V);
         LutPos pc = lut_pos<Q>(s[R_Cai], T.Cai);
 #define VR(col) lut_col<CV_NCOL>(T.V, pv, col)

@@ -38,6 +38,11 @@ struct MS {
         c.V_init = (float)r.vmin;
         return c;
     }
+    // no per-node parameters
+    static constexpr int kNodeParams = 0;
+    struct NodeG {};
+    __host__ __device__ static NodeG node_g(const C&, const float*, int64_t, int64_t) { return NodeG{}; }
+
     static int64_t table_floats(const double*) { return 0; }
     static Tables tables(const float*, const double*) { return Tables{}; }
 
@@ -48,7 +53,7 @@ struct MS {
 
     // ModifiedMS2v.differentiate (:36-44); returns dU and updates H
     template <class Q>
-    __host__ __device__ static float step(float U, float* s, const C& c, const Tables&) {
+    __host__ __device__ static float step(float U, float* s, const C& c, const Tables&, const NodeG&) {
         float H = s[0];
         float Uad = (U - c.vmin) / c.DV;
         float J_in = ((((-1.0f * H) * Uad) * (Uad - c.u_crit)) * (1.0f - Uad)) / c.tau_in;

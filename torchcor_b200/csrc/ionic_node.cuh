@@ -64,7 +64,7 @@ __device__ __forceinline__ void ionic_node(const MonoDev& d, const typename M::C
     float s[M::kStates];
 #pragma unroll
     for (int k = 0; k < M::kStates; ++k) s[k] = d.state[k * d.n_pad + i];
-    const float dV = M::template step<Q>(v, s, c, T);
+    const float dV = M::template step<Q>(v, s, c, T, M::node_g(c, d.node_params, d.n_pad, i));
 #pragma unroll
     for (int k = 0; k < M::kStates; ++k) d.state[k * d.n_pad + i] = s[k];
     // b = u*Cm + dt*du, du = dV/100  (monodomain.py:117-118)
@@ -144,7 +144,10 @@ __device__ __forceinline__ void ionic_group(const MonoDev& d, const typename M::
         }
         float b[V];
 #pragma unroll
-        for (int j = 0; j < V; ++j) b[j] = v[j] * d.cm + d.dt * Q::div(M::template step<Q>(v[j], s[j], c, T), 100.0f);
+        for (int j = 0; j < V; ++j)
+            b[j] = v[j] * d.cm +
+                   d.dt * Q::div(M::template step<Q>(v[j], s[j], c, T, M::node_g(c, d.node_params, d.n_pad, i0 + j)),
+                                 100.0f);
 #pragma unroll
         for (int k = 0; k < M::kStates; ++k) {
             float t[V];

@@ -55,6 +55,8 @@ struct TTP {
             pmf_INaK, KmNa, GbCa, GbNa, GpK, Gto, GK1, Vleak, Vmaxup, KupKup, Vxfer, invVcF_Cm, maxsr, dsr, EC,
             inverseVcF2, CAP, Vsr_Vc, BufcKbufc, Kbufc, k4, k2_, k1_, k3, Vrel, BufsrKbufsr, Kbufsr, Vc_Vss,
             Vsr_Vss, inverseVssF2, BufssKbufss, Kbufss, dt;
+        // per-node conductances from their arrays: ga1 = ((GCaL * Fconst) * F_RT) * 4, GKr * sqrt(Ko/5.4)
+        float Fconst, sqrt_Ko;
         // table constants
         float mdt, D_off, xr2c, mvHalf, nm1_FRT_dummy, n_, nm1, ksat, pmf_INaCa, Nao3, scl_tau_f;
         int endo;
@@ -91,6 +93,8 @@ struct TTP {
         c.halfFRT = (float)((1. / 2.) * F_RT);
         c.F_RT = (float)F_RT;
         c.GKr_sqrtKo = (float)r.GKr_init * (float)sqrt_Ko;
+        c.Fconst = (float)r.Fconst;
+        c.sqrt_Ko = (float)sqrt_Ko;
         c.GKs = (float)r.GKs_init;
         c.GNa = (float)r.GNa;
         c.pmf_INaK = (float)pmf_INaK;
@@ -150,6 +154,24 @@ struct TTP {
         for (int i = 0; i < TTP_NS; ++i) c.init[i] = (float)init[i];
         c.V_init = (float)r.V_init;
         return c;
+    }
+
+    // Per-node conductances (the reference's GCaL, GKr, GKs, Gto tensors,
+    // TenTusscherPanfilov.py:327-330): rows of tcb_mono.node_params when a caller
+    // set them node by node, else the uniform values of the parameters.
+    static constexpr int kNodeParams = 4;   // GCaL, GKr, GKs, Gto
+    struct NodeG {
+        float ga1, GKr_sqrtKo, GKs, Gto;
+    };
+    __host__ __device__ static NodeG node_g(const C& c, const float* np, int64_t n_pad, int64_t i) {
+        if (!np) return NodeG{c.ga1, c.GKr_sqrtKo, c.GKs, c.Gto};
+        NodeG g;
+        // ((GCaL * Fconst) * F_RT) * 4. and GKr * sqrt_Ko: float32 tensor times Python floats (:374, :377)
+        g.ga1 = ((np[i] * c.Fconst) * c.F_RT) * 4.0f;
+        g.GKr_sqrtKo = np[n_pad + i] * c.sqrt_Ko;
+        g.GKs = np[2 * n_pad + i];
+        g.Gto = np[3 * n_pad + i];
+        return g;
     }
 
     static int64_t table_floats(const double*) {
@@ -276,7 +298,7 @@ struct TTP {
     // The reference's order of operations; division and logarithm from the
     // policy Q (QFast or QExact, ionic_common.cuh).
     template <class Q>
-    __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T) {
+    __host__ __device__ static float step(float V, float* s, const C& c, const Tables& T, const NodeG& g) {
         LutPos pv = lut_pos<Q>(V, T.V);
         const float CaSR = s[S_CaSR], CaSS = s[S_CaSS], Cai = s[S_Cai], Ki = s[S_Ki], Nai = s[S_Nai];
         LutPos pc = lut_pos<Q>(CaSS, T.CaSS);
@@ -286,20 +308,20 @@ struct TTP {
         float Ena = c.RTONF * Q::log(Q::sdiv(c.Nao, Nai));
         float IpCa = Q::div(c.GpCa * Cai, Cai + c.KpCa);
         float v15 = V - 15.0f;
-        float a1 = c.ga1 * ((V == 15.0f) ? c.halfFRT : Q::div(v15, expm1f((2.0f * v15) * c.F_RT)));
+        float a1 = g.ga1 * ((V == 15.0f) ? c.halfFRT : Q::div(v15, expm1f((2.0f * v15) * c.F_RT)));
         const float2 a2_iNaK = lut_pair<TV_NCOL>(T.V, pv, TV_a2);  // TV_a2, TV_rec_iNaK
         float ICaL_A = a1 * a2_iNaK.x;
         float ICaL_B = a1 * c.Cao;
         float VmEk = V - Ek;
-        float IKr = ((c.GKr_sqrtKo * s[S_Xr1]) * s[S_Xr2]) * VmEk;
-        float IKs = ((c.GKs * s[S_Xs]) * s[S_Xs]) * (V - Eks);
+        float IKr = ((g.GKr_sqrtKo * s[S_Xr1]) * s[S_Xr2]) * VmEk;
+        float IKs = ((g.GKs * s[S_Xs]) * s[S_Xs]) * (V - Eks);
         float m = s[S_M];
         float INa = (((((c.GNa * m) * m) * m) * s[S_H]) * s[S_J]) * (V - Ena);
         float INaK = (c.pmf_INaK * Q::div(Nai, Nai + c.KmNa)) * a2_iNaK.y;
         float IbCa = c.GbCa * (V - Eca);
         float IbNa = c.GbNa * (V - Ena);
         float IpK = (c.GpK * lut_col<TV_NCOL>(T.V, pv, TV_rec_ipK)) * VmEk;
-        float Ito = ((c.Gto * s[S_R]) * s[S_S]) * VmEk;
+        float Ito = ((g.Gto * s[S_R]) * s[S_S]) * VmEk;
         LutPos pe = lut_pos<Q>(VmEk, T.VEk);
         float ICaL = (((s[S_D] * s[S_F]) * s[S_F2]) * s[S_FCaSS]) * ((ICaL_A * CaSS) - ICaL_B);
         const float2 naca = lut_pair<TV_NCOL>(T.V, pv, TV_INaCa_A);

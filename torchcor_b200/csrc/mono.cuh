@@ -19,6 +19,7 @@ struct MonoDev {
     float* state;
     const float* tables;
     float *x, *bp, *r, *p, *ap, *z, *p2, *at, *rt, *snap;
+    const float* node_params;   // per-node model parameters (n_params, n_pad), or null
     const uint32_t* stim_bits;
     const float* step_t;
     const uint32_t* step_stim;

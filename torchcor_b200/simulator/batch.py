@@ -55,6 +55,7 @@ class MonodomainBatch:
         n = len(self.sims)
         arr = (_lib.tcb_mono * n)()
         for i, s in enumerate(self.sims):
+            s._sync_node_params()
             arr[i] = s._sim["struct"]
         self._structs = arr
         lib = _lib.load()

@@ -219,12 +219,24 @@ class Monodomain:
         m.step_iters, m.counter = ptr(sim["step_iters"]), ptr(sim["counter"])
         m.scratch, m.barrier = ptr(sim["scratch"]), ptr(sim["barrier"])
         m.params = sim["params"].ctypes.data
+        m.node_params = ptr(im.node_params)
         sim["struct"] = m
         self._sim = sim
         return sim
 
+    def _sync_node_params(self):
+        """Point the device view at the model's per-node parameters once a caller has
+        set them node by node (e.g. TTP conductances after initialize(), as the
+        reference allows between steps)."""
+        rows = self.ionic_model.node_params
+        m = self._sim["struct"]
+        want = ptr(rows) if rows is not None else None
+        if (m.node_params or None) != want:
+            m.node_params = want
+
     def run_steps(self, n_steps, stream=None):
         """Advance the prepared simulation by ``n_steps`` steps (asynchronous)."""
+        self._sync_node_params()
         sim = self._sim
         a = sim["next_step"]
         b = min(a + n_steps, self.nt + 1)
@@ -252,6 +264,7 @@ class Monodomain:
     def capture_steps(self, n_steps):
         """Record ``n_steps`` steps of the prepared simulation in a CUDA graph;
         returns a callable replaying them (with the step bookkeeping)."""
+        self._sync_node_params()
         sim = self._sim
         lib = _lib.load()
         # the first launch on a device configures kernel attributes: keep it outside capture
