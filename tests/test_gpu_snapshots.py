@@ -2,7 +2,10 @@
 device, every frame copied to pinned host memory as soon as it is written; the
 frames, AT/RT and Vm.pt must be bit-identical to the default (every frame kept on
 the device), for rings smaller than the number of frames, one frame per step, and
-with node reordering."""
+with node reordering.  The default writes Vm.pt while the steps run
+(resultio.FrameWriter): its file must be torch.save's file of the frames."""
+import zipfile
+
 import numpy as np
 import pytest
 import torch
@@ -55,3 +58,47 @@ def test_graph_replay_equals_plain_launches(lib, cuda, tmp_path, name, interval,
     assert torch.equal(got.activation_time.cpu(), ref.activation_time.cpu())
     assert torch.equal(got.repolarization_time.cpu(), ref.repolarization_time.cpu())
     assert torch.equal(got._sim["step_iters"].cpu(), ref._sim["step_iters"].cpu())
+
+
+def test_frame_writer_follows_the_compute_stream(cuda, tmp_path):
+    from torchcor_b200.simulator.resultio import FrameWriter
+    g = torch.Generator(device=cuda).manual_seed(3)
+    src = torch.randn(9, 40_000, device=cuda, generator=g)
+    frames = torch.zeros_like(src)
+    w = FrameWriter(tmp_path / "Vm.pt", frames)
+    cur = torch.cuda.current_stream(cuda)
+    for k in range(src.shape[0] - 1):
+        torch.cuda._sleep(200_000)              # the frame is produced well after the mark is posted
+        frames[k].copy_(src[k] * 2.0)
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        w.produced(k + 1, ev)
+    frames[-1].copy_(src[-1] * 2.0)
+    ev = torch.cuda.Event()
+    ev.record(cur)
+    w.finish(ev)
+    assert torch.equal(torch.load(tmp_path / "Vm.pt"), (src * 2.0).cpu())
+    with zipfile.ZipFile(tmp_path / "Vm.pt") as z:
+        assert z.testzip() is None
+
+
+def test_frame_writer_abort_ends_the_thread(cuda, tmp_path):
+    from torchcor_b200.simulator.resultio import FrameWriter
+    frames = torch.zeros(4, 1000, device=cuda)
+    w = FrameWriter(tmp_path / "Vm.pt", frames)
+    ev = torch.cuda.Event()
+    ev.record()
+    w.produced(2, ev)
+    w.abort()
+    assert not w._thread.is_alive()
+    with pytest.raises(RuntimeError):
+        w.finish(ev)
+
+
+def test_solve_streams_vm_file_equal_to_saved_frames(lib, cuda, tmp_path):
+    case = C.case("cube6_ms_f32")
+    d = case_mesh_dir(case, tmp_path)
+    sim = _run(case, d, cuda, tmp_path / "a", None, 1.0)
+    with zipfile.ZipFile(tmp_path / "a" / "Vm.pt") as z:
+        assert z.testzip() is None
+    assert torch.equal(torch.load(tmp_path / "a" / "Vm.pt"), sim.solutions.cpu())

@@ -24,6 +24,7 @@ from torchcor_b200.core.conductivity import Conductivity
 from torchcor_b200.core.mesh import MeshReader
 from torchcor_b200.core.stimulation import Stimuli
 from torchcor_b200.device import get_device
+from torchcor_b200.simulator.resultio import FrameWriter
 
 
 def rcm_order(elems, n_nodes):
@@ -269,7 +270,8 @@ class Monodomain:
         lib = _lib.load()
         # the first launch on a device configures kernel attributes: keep it outside capture
         graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph):
+        # thread-local capture: a thread writing result files may use CUDA meanwhile
+        with torch.cuda.graph(graph, capture_error_mode="thread_local"):
             check(lib.tcb_mono_run(C.byref(sim["struct"]), 1, 1 + n_steps, stream_ptr()))
 
         def replay():
@@ -381,7 +383,18 @@ class Monodomain:
             if ev is not None:
                 torch.cuda.current_stream(self.device).wait_event(ev)
         check(lib.tcb_mono_finish(C.byref(st), stream_ptr()))
-        check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
+        writer = sim.pop("vm_writer", None)
+        if writer is not None:
+            done = torch.cuda.Event()
+            done.record(torch.cuda.current_stream(self.device))
+            try:
+                check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
+            except BaseException:
+                writer.abort()
+                raise
+            writer.finish(done)       # Vm.pt is complete
+        else:
+            check(lib.tcb_mono_check(C.byref(st), stream_ptr()))
         self.n_total_iter = int(sim["step_iters"].sum().item())
         self.activation_time = self._to_caller(sim["at"])
         self.repolarization_time = self._to_caller(sim["rt"])
@@ -396,7 +409,7 @@ class Monodomain:
             if calculate_AT_RT:
                 torch.save(self.activation_time.cpu(), rp / "ATs.pt")
                 torch.save(self.repolarization_time.cpu(), rp / "RTs.pt")
-            if self.solutions is not None:
+            if self.solutions is not None and writer is None:
                 torch.save(self.solutions.cpu(), rp / "Vm.pt")
         return self.n_total_iter
 
@@ -502,7 +515,8 @@ class Monodomain:
         return self.tuned
 
     def solve(self, a_tol, r_tol, max_iter, calculate_AT_RT=True, linear_guess=True, snapshot_interval=1,
-              verbose=True, result_path=None, snapshot_ring=None, graph_steps=100, autotune=True, launch=None):
+              verbose=True, result_path=None, snapshot_ring=None, graph_steps=100, autotune=True, launch=None,
+              stream_results=True):
         """monodomain.py:141-226.  ``snapshot_ring=R`` keeps only R snapshot frames on
         the device and streams every frame, as soon as it is written, into a pinned host
         tensor on a separate stream (``solutions`` is then that host tensor); the
@@ -512,7 +526,10 @@ class Monodomain:
         bit-identical to plain launches (``graph_steps=0``).  ``autotune`` picks the
         kernels' launch shapes first (``autotune()``; cached per device and shape);
         ``launch`` (a dict of ``ionic_variant``, ``cg_per_sm``, ``fused_step``) sets
-        them explicitly instead."""
+        them explicitly instead.  ``stream_results`` (default) writes ``Vm.pt`` while
+        the steps run: each frame goes from the device to its place in the file on a
+        thread of its own as soon as it is written (the same file as ``torch.save``
+        of the frames after the last step, which ``stream_results=False`` does)."""
         self.result_path = Path(result_path) if result_path is not None else None
         if self.result_path is not None:
             self.result_path.mkdir(parents=True, exist_ok=True)
@@ -528,24 +545,38 @@ class Monodomain:
             self.autotune()
         t0 = time.time()
         ring = sim["ring"]
+        writer = None
         if ring:
             self._snapshot_stream_init()
             chunk = max(1, sim["per_frame"])
         else:
             chunk = max(1, sim["per_frame"]) * (1 if verbose and snapshot_interval != self.T else 1000)
-        while sim["next_step"] <= self.nt:
-            n = min(chunk, self.nt + 1 - sim["next_step"])
-            if ring:
-                self._before_steps(sim["next_step"], n)
-            self._advance(n, graph_steps)
-            if ring:
-                self._drain_snapshots()
-            if verbose and snapshot_interval != self.T:
-                torch.cuda.synchronize(self.device)
-                done = sim["next_step"] - 1
-                print(f"t: {round(done * self.dt, 1)}/{self.T}", "Time elapsed:", round(time.time() - t0, 2),
-                      flush=True)
-        n_total_iter = self.finish(self.result_path if keep or calculate_AT_RT else None, calculate_AT_RT)
+            if stream_results and keep and self.result_path is not None and self._inv_t is None:
+                # Vm.pt is written while the steps run, frame by frame
+                writer = sim["vm_writer"] = FrameWriter(self.result_path / "Vm.pt", sim["snaps"])
+                chunk = max(1, sim["per_frame"])
+        try:
+            while sim["next_step"] <= self.nt:
+                n = min(chunk, self.nt + 1 - sim["next_step"])
+                if ring:
+                    self._before_steps(sim["next_step"], n)
+                self._advance(n, graph_steps)
+                if ring:
+                    self._drain_snapshots()
+                if writer is not None:
+                    ev = torch.cuda.Event()
+                    ev.record(torch.cuda.current_stream(self.device))
+                    writer.produced(self._frames_written() + 1, ev)
+                if verbose and snapshot_interval != self.T:
+                    torch.cuda.synchronize(self.device)
+                    done = sim["next_step"] - 1
+                    print(f"t: {round(done * self.dt, 1)}/{self.T}", "Time elapsed:", round(time.time() - t0, 2),
+                          flush=True)
+            n_total_iter = self.finish(self.result_path if keep or calculate_AT_RT else None, calculate_AT_RT)
+        except BaseException:
+            if sim.get("vm_writer") is not None:
+                sim.pop("vm_writer").abort()
+            raise
         elapsed = time.time() - t0
         if verbose:
             mem = torch.cuda.max_memory_allocated(self.device) / 1e9
