@@ -748,8 +748,9 @@ def main():
     ap.add_argument("--workload", default="ttp_cube", choices=["ttp_cube", "ms_cube", "batch_cubes", "serving"])
     ap.add_argument("--requests", type=int, default=128, help="serving: requests in the stream")
     ap.add_argument("--load", type=float, default=0.9, help="serving: offered load / capacity")
-    ap.add_argument("--capacity", type=float, default=3.5e9,
-                    help="serving: node-steps/s the arrival rate assumes (measured for this mix)")
+    ap.add_argument("--capacity", type=float, default=4.5e9,
+                    help="serving: node-steps/s the arrival rate assumes (the server's measured saturation "
+                         "for this mix on a B200)")
     ap.add_argument("--graph-steps", type=int, default=100,
                     help="steps per captured CUDA graph in the timed region (0 = plain launches)")
     ap.add_argument("--batch-graph-steps", type=int, default=50)

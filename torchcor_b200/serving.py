@@ -224,6 +224,10 @@ class Server:
         now = lambda: time.perf_counter() - t0   # noqa: E731
         tuned = not self.autotune
         self._staged = 0
+        # where the loop's time goes: host seconds building, waiting for the round,
+        # retiring and joining; device seconds of the batch steps (CUDA events)
+        spent = {"build_s": 0.0, "wait_s": 0.0, "retire_s": 0.0, "join_s": 0.0}
+        step_events = []
         while pending or self.active:
             if not self.active:
                 if pending[0].arrival_s > now():
@@ -238,29 +242,47 @@ class Server:
                 tuned = True
             k = min(self.round_steps, min(s.nt + 1 - s._sim["next_step"] for s in self.batch.sims))
             t1 = time.perf_counter()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(main)
             self.batch.step(max(1, k))
-            # build arrived requests on the side stream while the round runs
+            e1.record(main)
+            step_events.append((e0, e1))
+            # build arrived requests on the side stream while the round runs (a
+            # builder thread was measured slower: its kernels and its hold on the
+            # interpreter slowed the batch steps more than the overlap gained)
             staged = []
+            tb = time.perf_counter()
             with torch.cuda.stream(side):
                 while pending and pending[0].arrival_s <= now() and self._fits(pending[0]):
                     req = pending.popleft()
                     self.in_use += footprint_bytes(req)
                     self._staged += 1
                     staged.append((req, self._build(req, now)))
+            tw = time.perf_counter()
             side.synchronize()
             main.synchronize()
-            self.busy_s += time.perf_counter() - t1
+            tr = time.perf_counter()
+            self.busy_s += tr - t1
+            spent["build_s"] += tw - tb
+            spent["wait_s"] += tr - tw
             self.batch.check()
             for s in self.batch.finished():
                 self._retire(s, now)
+            tj = time.perf_counter()
             for req, sim in staged:
                 self._join(req, sim)
             self._staged = 0
+            spent["retire_s"] += tj - tr
+            spent["join_s"] += time.perf_counter() - tj
         wall = now()
+        torch.cuda.synchronize(self.device)
+        spent["steps_device_s"] = sum(a.elapsed_time(b) for a, b in step_events) / 1e3
+        spent["rounds"] = len(step_events)
         lat = np.array([r.latency_s for r in reqs])
         sim_ms = sum(r.T for r in reqs)
         return {"requests": len(reqs), "wall_s": wall, "node_steps": self.node_steps,
                 "node_steps_per_s": self.node_steps / wall, "simulated_ms_per_s": sim_ms / wall,
                 "requests_per_s": len(reqs) / wall,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-                "latency_mean_s": float(lat.mean()), "gpu_busy_frac": self.busy_s / wall}
+                "latency_mean_s": float(lat.mean()), "gpu_busy_frac": self.busy_s / wall,
+                "steps_device_frac": spent["steps_device_s"] / wall, "loop": spent}

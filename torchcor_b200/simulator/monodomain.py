@@ -108,8 +108,8 @@ class Monodomain:
     def load_arrays(self, nodes, elems, regions, fibres):
         """Mesh already in memory: nodes (N,3) in mm, elems (E,3|4), per-element regions and fibres."""
         self.n_nodes = int(nodes.shape[0])
-        elems = np.ascontiguousarray(elems, dtype=np.int32)
         if self.reorder:
+            elems = np.ascontiguousarray(elems, dtype=np.int32)
             perm = rcm_order(elems, self.n_nodes)
             inv = np.empty_like(perm)
             inv[perm] = np.arange(self.n_nodes, dtype=perm.dtype)
@@ -118,15 +118,21 @@ class Monodomain:
             self.node_order = perm
             self._perm_t = torch.from_numpy(perm).to(self.device)
             self._inv_t = torch.from_numpy(inv).to(self.device)
-        elems = np.ascontiguousarray(elems, dtype=np.int32)
-        self.nodes = torch.from_numpy(np.ascontiguousarray(nodes)).to(dtype=torch.float32, device=self.device)
-        self.elems = torch.from_numpy(elems).to(device=self.device)
+        self.nodes = self._upload(nodes, torch.float32)
+        self.elems = self._upload(elems, torch.int32)
         # the assembly pattern is built where the elements are (the device build on a GPU)
-        self._elems_np = self.elems if self.elems.is_cuda else elems
-        self.regions = torch.from_numpy(np.ascontiguousarray(regions)).to(dtype=torch.int, device=self.device)
-        self.fibres = torch.from_numpy(np.ascontiguousarray(fibres)).to(dtype=torch.float32, device=self.device)
+        self._elems_np = self.elems if self.elems.is_cuda else self.elems.numpy()
+        self.regions = self._upload(regions, torch.int)
+        self.fibres = self._upload(fibres, torch.float32)
         self.stimuli = Stimuli(self.n_nodes, self.device, self.dtype)
         self.conductivity = Conductivity(self.regions, dtype=self.dtype)
+
+    def _upload(self, a, dtype):
+        """Host array -> contiguous tensor of ``dtype`` on the device: the caller's
+        bytes are copied as they are and converted there (a mesh reader's int64
+        elements and float64 fibres would otherwise be converted on one host core)."""
+        t = torch.from_numpy(np.ascontiguousarray(a))
+        return t.to(self.device).to(dtype).contiguous()
 
     def _to_caller(self, t):
         """Per-node tensor (last axis) from the internal numbering to the caller's."""
