@@ -100,11 +100,42 @@ def test_batch_of_one_matches_single_path(lib, cuda, tmp_path):
     assert_close(c, outputs(s), *outputs(single))
 
 
+def test_batch_ionic_tiles_per_block_do_not_change_results(lib, cuda, tmp_path):
+    """The batched ionic launch's tiles per block (a tuning knob) only changes which
+    block updates which node: every choice gives the same bits."""
+    from torchcor_b200 import _lib
+    from torchcor_b200.simulator import MonodomainBatch
+    cases = [C.case(n) for n in MIX]
+    dirs = [case_mesh_dir(c, tmp_path) for c in cases]
+    results = {}
+    for tpb in (0, 1, 3, 16, 64):
+        batch = MonodomainBatch(cuda)
+        sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]) for c, d in zip(cases, dirs)]
+        batch.set_ionic(tpb)
+        assert batch.ionic_tiles_per_block == tpb
+        batch.run()
+        results[tpb] = [outputs(s) for s in sims]
+    for tpb, res in results.items():
+        for a, b in zip(res, results[0]):
+            assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3])) and a[3] == b[3], tpb
+    batch = MonodomainBatch(cuda)
+    with pytest.raises(ValueError):
+        batch.set_ionic(65)
+    batch.add(build(cases[0], dirs[0], cuda), cases[0]["tol"], cases[0]["tol"], cases[0]["max_iter"])
+    batch.cg_variants()                      # prepares the plan
+    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), -1) == _lib.TCB_EINVAL
+
+
+def C_byref(x):
+    import ctypes
+    return ctypes.byref(x)
+
+
 def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
     """The tuner times real steps of the batch with each CG variant, keeps the
     fastest, caches it, and the simulations still match the reference."""
     from torchcor_b200.simulator import MonodomainBatch
-    from torchcor_b200.tune import CG_VARIANTS, TuneCache, tune_batch
+    from torchcor_b200.tune import BATCH_IONIC_TPB, CG_VARIANTS, TuneCache, tune_batch
     cases = [C.case(n) for n in ("cube6_ms_f32", "cube8_ttp_f32")]
     dirs = [case_mesh_dir(c, tmp_path) for c in cases]
     cache = TuneCache(tmp_path / "tune.json")
@@ -113,9 +144,14 @@ def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
     choice, times = tune_batch(batch, steps=3, cache=cache)
     assert choice in CG_VARIANTS and set(times) == set(batch.cg_variants())
     assert batch.cg_config[0] == choice
-    assert len(cache.load()) == 1
+    entry = next(iter(cache.load().values()))
+    assert len(cache.load()) == 1 and entry["ionic_tiles_per_block"] in BATCH_IONIC_TPB
+    assert batch.ionic_tiles_per_block == entry["ionic_tiles_per_block"]
+    assert set(entry["ionic_ms_per_step"]) == {str(t) for t in BATCH_IONIC_TPB}
+    batch.set_ionic(0)
     again, t2 = tune_batch(batch, steps=3, cache=cache)
     assert again == choice and t2 is None          # served from the cache
+    assert batch.ionic_tiles_per_block == entry["ionic_tiles_per_block"]
     batch.run()
     for c, s in zip(cases, sims):
         g = golden(c["name"])

@@ -55,8 +55,10 @@ struct BatchWS {
     BatchGroup groups[kBatchGroups];
 };
 
+constexpr int kBatchMaxTilesPerBlock = 64;   // tcb_batch_set_ionic's upper limit
 int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* models, const int64_t* tiles,
-                           const int32_t* shared, const char (*consts)[1024], cudaStream_t s);
+                           const int32_t* shared, const char (*consts)[1024], int tiles_per_block,
+                           cudaStream_t s);
 // batched CG variants: 1 / 2 = streaming, sized for 1 / 2 blocks per SM;
 // 3 = ELL streams staged in shared memory by bulk copies, 1 block per SM
 // flags: the (int16 columns 4, A rebuilt 2, linear guess 1) combination all the

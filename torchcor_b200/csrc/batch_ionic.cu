@@ -190,7 +190,8 @@ int model_tables_view(int model, const float* tables, const double* params, void
 }
 
 int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* models, const int64_t* tiles,
-                           const int32_t* shared, const char (*consts)[1024], cudaStream_t s) {
+                           const int32_t* shared, const char (*consts)[1024], int tiles_per_block,
+                           cudaStream_t s) {
     static_assert(sizeof(IonicLaunch) <= 4000, "kernel argument block");
     IonicLaunch P;
     memset(&P, 0, sizeof P);
@@ -208,8 +209,10 @@ int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* m
     int64_t blocks = 0;
     for (int k = 0; k < n; ++k) {
         const int g = order[k];
+        // tiles per block: the plan's choice (a tuning knob), else sized from the group
         const int64_t per = (tiles[g] + (int64_t)sms * kBlocksPerSmTarget - 1) / ((int64_t)sms * kBlocksPerSmTarget);
-        const int tpb = (int)(per < 1 ? 1 : per > kMaxTilesPerBlock ? kMaxTilesPerBlock : per);
+        const int tpb = tiles_per_block > 0 ? tiles_per_block
+                                            : (int)(per < 1 ? 1 : per > kMaxTilesPerBlock ? kMaxTilesPerBlock : per);
         P.group[k] = g;
         P.tpb[k] = tpb;
         P.shared[k] = shared[g];

@@ -31,6 +31,7 @@ class MonodomainBatch:
         self.sims = []
         self._dirty = True
         self._cg_variant = None
+        self._ionic_tpb = 0
 
     def add(self, sim, a_tol=1e-5, r_tol=1e-5, max_iter=100, calculate_AT_RT=True, linear_guess=True,
             snapshot_interval=1):
@@ -66,6 +67,8 @@ class MonodomainBatch:
                 self._cg_variant = None
             else:
                 check(st)
+        if self._ionic_tpb:
+            check(lib.tcb_batch_set_ionic(C.byref(self._plan), int(self._ionic_tpb)))
         self._dirty = False
 
     def set_cg(self, variant):
@@ -76,6 +79,20 @@ class MonodomainBatch:
         self._cg_variant = variant
         if self.sims and not self._dirty:
             check(_lib.load().tcb_batch_set_cg(C.byref(self._plan), int(variant)))
+
+    def set_ionic(self, tiles_per_block):
+        """Tiles of 128 nodes each block of the batched ionic launch walks: 0 (sized
+        from the model groups, the default) or 1..64."""
+        tpb = int(tiles_per_block)
+        if not 0 <= tpb <= 64:
+            raise ValueError("tiles_per_block must be in 0..64")
+        self._ionic_tpb = tpb
+        if self.sims and not self._dirty:
+            check(_lib.load().tcb_batch_set_ionic(C.byref(self._plan), tpb))
+
+    @property
+    def ionic_tiles_per_block(self):
+        return self._ionic_tpb
 
     def cg_variants(self):
         """The CG variants this batch can use (3 needs 16-byte aligned ELL arrays)."""

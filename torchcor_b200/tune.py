@@ -86,14 +86,18 @@ def batch_key(device, n_nodes, models) -> str:
     return f"batch_cg|{device_key(device)}|{batch_signature(n_nodes, models)}"
 
 
+BATCH_IONIC_TPB = (0, 1, 2, 4, 8, 16)   # batched ionic tiles per block (0: sized from the groups)
+
+
 def tune_batch(batch, steps=10, cache=None, force=False):
-    """Pick the batched CG variant for ``batch`` (a prepared ``MonodomainBatch``).
+    """Pick the batched CG variant and then the batched ionic launch's tiles per
+    block for ``batch`` (a prepared ``MonodomainBatch``).
 
     Uses the cached choice when there is one (unless ``force``); otherwise runs
     ``steps`` real batch steps with each candidate after one untimed step, keeps
-    the fastest and records it.  Needs ``(steps + 1) * len(candidates)`` steps
-    left in every simulation; with fewer it keeps the default and records
-    nothing.  Returns ``(variant, timings_ms_per_step or None)``."""
+    the fastest of each and records them.  Needs ``(steps + 1) x`` (number of
+    candidates) steps left in every simulation; with fewer it keeps the defaults
+    and records nothing.  Returns ``(variant, timings_ms_per_step or None)``."""
     cache = cache if cache is not None else TuneCache()
     sims = batch.sims
     if not sims:
@@ -103,15 +107,15 @@ def tune_batch(batch, steps=10, cache=None, force=False):
     if hit is not None:
         if int(hit["cg_variant"]) in batch.cg_variants():
             batch.set_cg(int(hit["cg_variant"]))
+            batch.set_ionic(int(hit.get("ionic_tiles_per_block", 0)))
             return int(hit["cg_variant"]), None
     candidates = batch.cg_variants()
-    need = (steps + 1) * len(candidates)
+    need = (steps + 1) * (len(candidates) + len(BATCH_IONIC_TPB))
     if min(s.nt + 1 - s._sim["next_step"] for s in sims) < need:
         return batch.cg_config[0], None
     stream = torch.cuda.current_stream(batch.device)
-    times = {}
-    for v in candidates:
-        batch.set_cg(v)
+
+    def timed():
         batch.step(1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -119,10 +123,23 @@ def tune_batch(batch, steps=10, cache=None, force=False):
         e1.record(stream)
         e1.synchronize()
         batch.check()
-        times[v] = e0.elapsed_time(e1) / steps
+        return e0.elapsed_time(e1) / steps
+
+    times = {}
+    for v in candidates:
+        batch.set_cg(v)
+        times[v] = timed()
     best = min(times, key=times.get)
     batch.set_cg(best)
-    cache.put(key, {"cg_variant": best, "ms_per_step": {str(k): v for k, v in times.items()}})
+    tpb_times = {}
+    for t in BATCH_IONIC_TPB:
+        batch.set_ionic(t)
+        tpb_times[t] = timed()
+    tpb = min(tpb_times, key=tpb_times.get)
+    batch.set_ionic(tpb)
+    cache.put(key, {"cg_variant": best, "ms_per_step": {str(k): v for k, v in times.items()},
+                    "ionic_tiles_per_block": tpb,
+                    "ionic_ms_per_step": {str(k): v for k, v in tpb_times.items()}})
     return best, times
 
 
