@@ -298,6 +298,8 @@ typedef struct tcb_batch_plan {
     int32_t ionic_tiles_per_block;   /* batched ionic kernel: 128-node tiles each block walks;
                                         0 = sized from each model group (at most 8, at least
                                         16 blocks per SM where the group is large enough) */
+    int32_t ionic_blocks_per_sm;     /* its register budget: 4, 6, 8 or 12 blocks of 128
+                                        threads per SM; 0 = 8 with CRN groups, else 12 */
 } tcb_batch_plan;
 
 int64_t tcb_batch_workspace_bytes(int32_t n_sims);
@@ -307,10 +309,12 @@ int tcb_batch_prepare(const tcb_mono* sims, int32_t n_sims, void* workspace, int
  * do not allow bulk copies.  No counterpart in the reference (a tuning knob of
  * this implementation). */
 int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant);
-/* Tiles per block of the plan's batched ionic launch: 0 (sized from the groups, the
- * default after tcb_batch_prepare) or 1..64 for every group.  TCB_EINVAL outside that
- * range.  No counterpart in the reference (a tuning knob of this implementation). */
-int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block);
+/* The plan's batched ionic launch: tiles per block, 0 (sized from the groups, the
+ * default after tcb_batch_prepare) or 1..64 for every group, and the kernel instance's
+ * register budget, 0 (default) or 4, 6, 8, 12 blocks per SM.  TCB_EINVAL otherwise.
+ * Results do not depend on either.  No counterpart in the reference (tuning knobs of
+ * this implementation). */
+int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block, int32_t blocks_per_sm);
 /* `steps` batch steps: every listed simulation whose counter is in [1, nt] advances one step each. */
 int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream);
 /* Device error word of the batch (synchronises the stream). */

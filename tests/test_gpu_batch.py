@@ -108,22 +108,25 @@ def test_batch_ionic_tiles_per_block_do_not_change_results(lib, cuda, tmp_path):
     cases = [C.case(n) for n in MIX]
     dirs = [case_mesh_dir(c, tmp_path) for c in cases]
     results = {}
-    for tpb in (0, 1, 3, 16, 64):
+    for tpb, bps in ((0, 0), (1, 4), (3, 6), (16, 8), (64, 12), (0, 12)):
         batch = MonodomainBatch(cuda)
         sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]) for c, d in zip(cases, dirs)]
-        batch.set_ionic(tpb)
-        assert batch.ionic_tiles_per_block == tpb
+        batch.set_ionic(tpb, bps)
+        assert (batch.ionic_tiles_per_block, batch.ionic_blocks_per_sm) == (tpb, bps)
         batch.run()
-        results[tpb] = [outputs(s) for s in sims]
+        results[(tpb, bps)] = [outputs(s) for s in sims]
     for tpb, res in results.items():
-        for a, b in zip(res, results[0]):
+        for a, b in zip(res, results[(0, 0)]):
             assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3])) and a[3] == b[3], tpb
     batch = MonodomainBatch(cuda)
     with pytest.raises(ValueError):
         batch.set_ionic(65)
+    with pytest.raises(ValueError):
+        batch.set_ionic(0, 5)
     batch.add(build(cases[0], dirs[0], cuda), cases[0]["tol"], cases[0]["tol"], cases[0]["max_iter"])
     batch.cg_variants()                      # prepares the plan
-    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), -1) == _lib.TCB_EINVAL
+    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), -1, 0) == _lib.TCB_EINVAL
+    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), 0, 7) == _lib.TCB_EINVAL
 
 
 def C_byref(x):
@@ -135,7 +138,7 @@ def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
     """The tuner times real steps of the batch with each CG variant, keeps the
     fastest, caches it, and the simulations still match the reference."""
     from torchcor_b200.simulator import MonodomainBatch
-    from torchcor_b200.tune import BATCH_IONIC_TPB, CG_VARIANTS, TuneCache, tune_batch
+    from torchcor_b200.tune import BATCH_IONIC_BPS, BATCH_IONIC_TPB, CG_VARIANTS, TuneCache, tune_batch
     cases = [C.case(n) for n in ("cube6_ms_f32", "cube8_ttp_f32")]
     dirs = [case_mesh_dir(c, tmp_path) for c in cases]
     cache = TuneCache(tmp_path / "tune.json")
@@ -148,7 +151,9 @@ def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
     assert len(cache.load()) == 1 and entry["ionic_tiles_per_block"] in BATCH_IONIC_TPB
     assert batch.ionic_tiles_per_block == entry["ionic_tiles_per_block"]
     assert set(entry["ionic_ms_per_step"]) == {str(t) for t in BATCH_IONIC_TPB}
-    batch.set_ionic(0)
+    assert entry["ionic_blocks_per_sm"] in BATCH_IONIC_BPS
+    assert batch.ionic_blocks_per_sm == entry["ionic_blocks_per_sm"]
+    batch.set_ionic(0, 0)
     again, t2 = tune_batch(batch, steps=3, cache=cache)
     assert again == choice and t2 is None          # served from the cache
     assert batch.ionic_tiles_per_block == entry["ionic_tiles_per_block"]

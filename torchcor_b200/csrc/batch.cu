@@ -230,6 +230,7 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
     plan->cg_smem = (int32_t)smem;
     plan->total_slices = S;
     plan->ionic_tiles_per_block = 0;
+    plan->ionic_blocks_per_sm = 0;
     return TCB_OK;
 }
 
@@ -248,10 +249,13 @@ extern "C" int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant) {
     return TCB_OK;
 }
 
-extern "C" int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block) {
+extern "C" int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block, int32_t blocks_per_sm) {
     if (!plan || !plan->workspace || tiles_per_block < 0 || tiles_per_block > kBatchMaxTilesPerBlock)
         return fail(TCB_EINVAL, "tcb_batch_set_ionic: tiles per block outside 0..64");
+    if (!batch_ionic_blocks_ok(blocks_per_sm))
+        return fail(TCB_EINVAL, "tcb_batch_set_ionic: blocks per SM not 0, 4, 6, 8 or 12");
     plan->ionic_tiles_per_block = tiles_per_block;
+    plan->ionic_blocks_per_sm = blocks_per_sm;
     return TCB_OK;
 }
 
@@ -261,13 +265,15 @@ extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* st
         (plan->cg_variant == 3 && (!plan->cg_stage_ok || plan->cg_stage_bytes < 2048)) || plan->cg_flags < -1 ||
         plan->cg_flags > 7)
         return fail(TCB_EINVAL, "tcb_batch_run: plan CG grid out of range");
-    if (plan->ionic_tiles_per_block < 0 || plan->ionic_tiles_per_block > kBatchMaxTilesPerBlock)
-        return fail(TCB_EINVAL, "tcb_batch_run: plan ionic tiles per block out of range");
+    if (plan->ionic_tiles_per_block < 0 || plan->ionic_tiles_per_block > kBatchMaxTilesPerBlock ||
+        !batch_ionic_blocks_ok(plan->ionic_blocks_per_sm))
+        return fail(TCB_EINVAL, "tcb_batch_run: plan ionic launch out of range");
     cudaStream_t s = as_stream(stream);
     const BatchWS* W = static_cast<const BatchWS*>(plan->workspace);
     for (int64_t k = 0; k < steps; ++k) {
         int st = launch_batch_ionic_all(W, plan->n_groups, plan->group_model, plan->group_tiles, plan->group_shared,
-                                        plan->group_consts, plan->ionic_tiles_per_block, s);
+                                        plan->group_consts, plan->ionic_tiles_per_block,
+                                        plan->ionic_blocks_per_sm, s);
         if (st) return st;
         st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_variant, plan->cg_stage_bytes,
                              plan->cg_flags, s);

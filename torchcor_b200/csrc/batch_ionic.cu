@@ -102,14 +102,15 @@ __device__ __forceinline__ void run_group(const IonicLaunch& P, int k, int64_t b
 }
 
 // One launch for the ionic step of every simulation of the batch: blocks
-// [block_prefix[k], block_prefix[k+1]) run the k-th group's model.  Two
-// instances: a batch with CRN groups runs the one with every model, compiled for
-// 8 blocks per SM (64 registers), where CRN's state spills least; a batch without
-// runs the one without the CRN path, compiled for 12 (40 registers).  Measured on
-// B200: 64 MS/TTP cubes 0.730 -> 0.714 ms a step; a CRN-heavy batch is 6 % slower
-// at 12 blocks per SM than at 8, so the instance with CRN stays at 8.
-template <bool WITH_CRN>
-__global__ void __launch_bounds__(kThreads, WITH_CRN ? 8 : 12) batch_ionic_kernel(const IonicLaunch P) {
+// [block_prefix[k], block_prefix[k+1]) run the k-th group's model.  A batch with
+// CRN groups runs an instance with every model, a batch without one without the
+// CRN path; each is compiled for MINB = 4, 6, 8 or 12 blocks of 128 threads per SM
+// (128, 80, 64 or 40 registers).  The defaults (no choice in the plan): 8 with
+// CRN, where its state spills least, 12 without (measured on B200: 64 MS/TTP cubes
+// 0.730 -> 0.714 ms a step at 12; a CRN-heavy batch 6 % slower at 12 than at 8);
+// the batch tuner times the others.
+template <bool WITH_CRN, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) batch_ionic_kernel(const IonicLaunch P) {
     __shared__ MonoDev sd;
     __shared__ __align__(16) unsigned char tabs[kTablesBytes];
     __shared__ int s_lo;
@@ -189,9 +190,22 @@ int model_tables_view(int model, const float* tables, const double* params, void
     return fail(TCB_EINVAL, "unknown ionic model");
 }
 
+template <bool WITH_CRN>
+int launch_ionic_instance(const IonicLaunch& P, unsigned blocks, int blocks_per_sm, cudaStream_t s) {
+    switch (blocks_per_sm) {
+        case 4: batch_ionic_kernel<WITH_CRN, 4><<<blocks, kThreads, 0, s>>>(P); break;
+        case 6: batch_ionic_kernel<WITH_CRN, 6><<<blocks, kThreads, 0, s>>>(P); break;
+        case 8: batch_ionic_kernel<WITH_CRN, 8><<<blocks, kThreads, 0, s>>>(P); break;
+        case 12: batch_ionic_kernel<WITH_CRN, 12><<<blocks, kThreads, 0, s>>>(P); break;
+        default: return fail(TCB_EINVAL, "batched ionic kernel: blocks per SM not 4, 6, 8 or 12");
+    }
+    TCB_CHECK_LAUNCH("batched ionic kernel");
+    return TCB_OK;
+}
+
 int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* models, const int64_t* tiles,
                            const int32_t* shared, const char (*consts)[1024], int tiles_per_block,
-                           cudaStream_t s) {
+                           int blocks_per_sm, cudaStream_t s) {
     static_assert(sizeof(IonicLaunch) <= 4000, "kernel argument block");
     IonicLaunch P;
     memset(&P, 0, sizeof P);
@@ -231,10 +245,8 @@ int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* m
     P.block_prefix[n] = blocks;
     if (blocks < 1) return TCB_OK;
     if (blocks > INT32_MAX) return fail(TCB_ERANGE, "batched ionic grid too large");
-    if (with_crn) batch_ionic_kernel<true><<<(unsigned)blocks, kThreads, 0, s>>>(P);
-    else batch_ionic_kernel<false><<<(unsigned)blocks, kThreads, 0, s>>>(P);
-    TCB_CHECK_LAUNCH("batched ionic kernel");
-    return TCB_OK;
+    if (with_crn) return launch_ionic_instance<true>(P, (unsigned)blocks, blocks_per_sm > 0 ? blocks_per_sm : 8, s);
+    return launch_ionic_instance<false>(P, (unsigned)blocks, blocks_per_sm > 0 ? blocks_per_sm : 12, s);
 }
 
 }  // namespace tcb

@@ -32,6 +32,7 @@ class MonodomainBatch:
         self._dirty = True
         self._cg_variant = None
         self._ionic_tpb = 0
+        self._ionic_bps = 0
 
     def add(self, sim, a_tol=1e-5, r_tol=1e-5, max_iter=100, calculate_AT_RT=True, linear_guess=True,
             snapshot_interval=1):
@@ -67,8 +68,8 @@ class MonodomainBatch:
                 self._cg_variant = None
             else:
                 check(st)
-        if self._ionic_tpb:
-            check(lib.tcb_batch_set_ionic(C.byref(self._plan), int(self._ionic_tpb)))
+        if self._ionic_tpb or self._ionic_bps:
+            check(lib.tcb_batch_set_ionic(C.byref(self._plan), int(self._ionic_tpb), int(self._ionic_bps)))
         self._dirty = False
 
     def set_cg(self, variant):
@@ -80,19 +81,28 @@ class MonodomainBatch:
         if self.sims and not self._dirty:
             check(_lib.load().tcb_batch_set_cg(C.byref(self._plan), int(variant)))
 
-    def set_ionic(self, tiles_per_block):
-        """Tiles of 128 nodes each block of the batched ionic launch walks: 0 (sized
-        from the model groups, the default) or 1..64."""
-        tpb = int(tiles_per_block)
+    def set_ionic(self, tiles_per_block=None, blocks_per_sm=None):
+        """The batched ionic launch: tiles of 128 nodes each block walks, 0 (sized
+        from the model groups, the default) or 1..64, and the kernel instance's
+        register budget, 0 (default: 8 blocks of 128 threads per SM with CRN
+        simulations, else 12) or 4, 6, 8, 12.  ``None`` keeps the current value."""
+        tpb = self._ionic_tpb if tiles_per_block is None else int(tiles_per_block)
+        bps = self._ionic_bps if blocks_per_sm is None else int(blocks_per_sm)
         if not 0 <= tpb <= 64:
             raise ValueError("tiles_per_block must be in 0..64")
-        self._ionic_tpb = tpb
+        if bps not in (0, 4, 6, 8, 12):
+            raise ValueError("blocks_per_sm must be 0, 4, 6, 8 or 12")
+        self._ionic_tpb, self._ionic_bps = tpb, bps
         if self.sims and not self._dirty:
-            check(_lib.load().tcb_batch_set_ionic(C.byref(self._plan), tpb))
+            check(_lib.load().tcb_batch_set_ionic(C.byref(self._plan), tpb, bps))
 
     @property
     def ionic_tiles_per_block(self):
         return self._ionic_tpb
+
+    @property
+    def ionic_blocks_per_sm(self):
+        return self._ionic_bps
 
     def cg_variants(self):
         """The CG variants this batch can use (3 needs 16-byte aligned ELL arrays)."""

@@ -87,11 +87,12 @@ def batch_key(device, n_nodes, models) -> str:
 
 
 BATCH_IONIC_TPB = (0, 1, 2, 4, 8, 16)   # batched ionic tiles per block (0: sized from the groups)
+BATCH_IONIC_BPS = (0, 4, 6, 8, 12)      # its register budget in blocks per SM (0: the default)
 
 
 def tune_batch(batch, steps=10, cache=None, force=False):
-    """Pick the batched CG variant and then the batched ionic launch's tiles per
-    block for ``batch`` (a prepared ``MonodomainBatch``).
+    """Pick the batched CG variant, then the batched ionic launch's tiles per block,
+    then its register budget, for ``batch`` (a prepared ``MonodomainBatch``).
 
     Uses the cached choice when there is one (unless ``force``); otherwise runs
     ``steps`` real batch steps with each candidate after one untimed step, keeps
@@ -107,10 +108,10 @@ def tune_batch(batch, steps=10, cache=None, force=False):
     if hit is not None:
         if int(hit["cg_variant"]) in batch.cg_variants():
             batch.set_cg(int(hit["cg_variant"]))
-            batch.set_ionic(int(hit.get("ionic_tiles_per_block", 0)))
+            batch.set_ionic(int(hit.get("ionic_tiles_per_block", 0)), int(hit.get("ionic_blocks_per_sm", 0)))
             return int(hit["cg_variant"]), None
     candidates = batch.cg_variants()
-    need = (steps + 1) * (len(candidates) + len(BATCH_IONIC_TPB))
+    need = (steps + 1) * (len(candidates) + len(BATCH_IONIC_TPB) + len(BATCH_IONIC_BPS))
     if min(s.nt + 1 - s._sim["next_step"] for s in sims) < need:
         return batch.cg_config[0], None
     stream = torch.cuda.current_stream(batch.device)
@@ -133,13 +134,21 @@ def tune_batch(batch, steps=10, cache=None, force=False):
     batch.set_cg(best)
     tpb_times = {}
     for t in BATCH_IONIC_TPB:
-        batch.set_ionic(t)
+        batch.set_ionic(tiles_per_block=t)
         tpb_times[t] = timed()
     tpb = min(tpb_times, key=tpb_times.get)
-    batch.set_ionic(tpb)
+    batch.set_ionic(tiles_per_block=tpb)
+    bps_times = {}
+    for b in BATCH_IONIC_BPS:
+        batch.set_ionic(blocks_per_sm=b)
+        bps_times[b] = timed()
+    bps = min(bps_times, key=bps_times.get)
+    batch.set_ionic(blocks_per_sm=bps)
     cache.put(key, {"cg_variant": best, "ms_per_step": {str(k): v for k, v in times.items()},
                     "ionic_tiles_per_block": tpb,
-                    "ionic_ms_per_step": {str(k): v for k, v in tpb_times.items()}})
+                    "ionic_ms_per_step": {str(k): v for k, v in tpb_times.items()},
+                    "ionic_blocks_per_sm": bps,
+                    "ionic_budget_ms_per_step": {str(k): v for k, v in bps_times.items()}})
     return best, times
 
 
