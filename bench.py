@@ -597,7 +597,7 @@ def batch_arm(a, world, rank, local, clk, steps=None):
         tuned = tune_batch(batch, steps=10)[1]
         torch.cuda.synchronize(dev)
     cg_cfg = batch.cg_config
-    ionic_tpb, ionic_bps = batch.ionic_tiles_per_block, batch.ionic_blocks_per_sm
+    ionic_tpb, ionic_bps, ionic_staged = batch.ionic_tiles_per_block, batch.ionic_blocks_per_sm, batch.ionic_staged
     # the timed steps replay CUDA graphs of G steps, the remainder runs as plain launches
     G = a.batch_graph_steps if 0 < a.batch_graph_steps <= K else 0
     replay = batch.capture(G) if G else None
@@ -691,6 +691,7 @@ def batch_arm(a, world, rank, local, clk, steps=None):
                                   f"Mitchell-Schaeffer/TTP ENDO 50/50, dt 0.01 ms",
                       "simulations": len(wls), "nodes": total, "cg_variant": cg_cfg[0], "cg_blocks": cg_cfg[1],
                       "ionic_tiles_per_block": ionic_tpb, "ionic_blocks_per_sm": ionic_bps,
+                      "ionic_staged": ionic_staged,
                       "autotune_ms_per_step": tuned, "cg_iterations_per_step":
                           float(its.sum().item()) / K / len(wls),
                       "cg_passes_per_step": passes_max, "cg_passes_per_node_step": passes_node,

@@ -299,7 +299,12 @@ typedef struct tcb_batch_plan {
                                         0 = sized from each model group (at most 8, at least
                                         16 blocks per SM where the group is large enough) */
     int32_t ionic_blocks_per_sm;     /* its register budget: 4, 6, 8 or 12 blocks of 128
-                                        threads per SM; 0 = 8 with CRN groups, else 12 */
+                                        threads per SM; 0 = 8 with CRN groups, else 12 (the
+                                        staged form: 4, 6 or 8; 0 = 6) */
+    int32_t ionic_staged;            /* 1: the staged form (each block's next tile copied into
+                                        shared memory by bulk copies while it computes one) */
+    int32_t ionic_stage_ok;          /* 1 if every per-node array allows bulk copies (16-byte
+                                        aligned) */
 } tcb_batch_plan;
 
 int64_t tcb_batch_workspace_bytes(int32_t n_sims);
@@ -310,11 +315,14 @@ int tcb_batch_prepare(const tcb_mono* sims, int32_t n_sims, void* workspace, int
  * this implementation). */
 int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant);
 /* The plan's batched ionic launch: tiles per block, 0 (sized from the groups, the
- * default after tcb_batch_prepare) or 1..64 for every group, and the kernel instance's
- * register budget, 0 (default) or 4, 6, 8, 12 blocks per SM.  TCB_EINVAL otherwise.
- * Results do not depend on either.  No counterpart in the reference (tuning knobs of
- * this implementation). */
-int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block, int32_t blocks_per_sm);
+ * default after tcb_batch_prepare) or 1..64 for every group; the kernel instance's
+ * register budget, 0 (default) or 4, 6, 8, 12 blocks per SM (4, 6, 8 staged); staged
+ * 0 or 1 (TCB_ERANGE if the arrays do not allow it, see ionic_stage_ok).  TCB_EINVAL for
+ * other values.  The staged form takes the single-simulation default's division policy
+ * (hardware division for TTP and CRN), so its results differ from the unstaged form's
+ * by rounding only; tiles and budget do not change results.  No counterpart in the
+ * reference (tuning knobs of this implementation). */
+int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block, int32_t blocks_per_sm, int32_t staged);
 /* `steps` batch steps: every listed simulation whose counter is in [1, nt] advances one step each. */
 int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* stream);
 /* Device error word of the batch (synchronises the stream). */

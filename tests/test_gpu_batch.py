@@ -125,8 +125,46 @@ def test_batch_ionic_tiles_per_block_do_not_change_results(lib, cuda, tmp_path):
         batch.set_ionic(0, 5)
     batch.add(build(cases[0], dirs[0], cuda), cases[0]["tol"], cases[0]["tol"], cases[0]["max_iter"])
     batch.cg_variants()                      # prepares the plan
-    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), -1, 0) == _lib.TCB_EINVAL
-    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), 0, 7) == _lib.TCB_EINVAL
+    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), -1, 0, 0) == _lib.TCB_EINVAL
+    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), 0, 7, 0) == _lib.TCB_EINVAL
+    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), 0, 12, 1) == _lib.TCB_EINVAL
+    assert _lib.load().tcb_batch_set_ionic(C_byref(batch._plan), 0, 0, 2) == _lib.TCB_EINVAL
+
+
+def test_batch_staged_ionic_matches_alone_and_reference(lib, cuda, tmp_path):
+    """The staged batched ionic form (bulk copies of each block's next tile, the
+    single-simulation default's division policy) against the simulations alone and
+    the reference fixtures, at each register budget; tiles per block do not change
+    its bits."""
+    from torchcor_b200.simulator import MonodomainBatch
+    cases = [C.case(n) for n in MIX]
+    dirs = [case_mesh_dir(c, tmp_path) for c in cases]
+    alone = []
+    for c, d in zip(cases, dirs):
+        s = build(c, d, cuda)
+        s.solve(c["tol"], c["tol"], c["max_iter"], verbose=False)
+        alone.append(outputs(s))
+    bits = {}
+    for tpb, bps in ((0, 4), (0, 6), (0, 8), (2, 6)):
+        batch = MonodomainBatch(cuda)
+        sims = [batch.add(build(c, d, cuda), c["tol"], c["tol"], c["max_iter"]) for c, d in zip(cases, dirs)]
+        assert batch.ionic_stage_ok()
+        batch.set_ionic(tpb, bps, staged=True)
+        assert batch.ionic_staged == 1
+        batch.run()
+        got_all = [outputs(s) for s in sims]
+        for c, got, a in zip(cases, got_all, alone):
+            assert_close(c, got, *a)
+            g = golden(c["name"])
+            vm = got[2] if "Vm_idx" not in g else got[2][g["Vm_idx"]]
+            assert_close(c, (got[0], got[1], vm, got[3]), g["AT"], g["RT"], g["Vm"], int(g["n_total_iter"]))
+        bits.setdefault(bps, got_all)
+        if (tpb, bps) == (2, 6):
+            for a, b in zip(got_all, bits[6]):
+                assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3])) and a[3] == b[3]
+    batch = MonodomainBatch(cuda)
+    with pytest.raises(ValueError):
+        batch.set_ionic(0, 12, staged=True)       # no 12-block budget for the staged form
 
 
 def C_byref(x):
@@ -153,10 +191,13 @@ def test_batch_autotune_choice_is_cached_and_results_hold(lib, cuda, tmp_path):
     assert set(entry["ionic_ms_per_step"]) == {str(t) for t in BATCH_IONIC_TPB}
     assert entry["ionic_blocks_per_sm"] in BATCH_IONIC_BPS
     assert batch.ionic_blocks_per_sm == entry["ionic_blocks_per_sm"]
-    batch.set_ionic(0, 0)
+    assert batch.ionic_staged == entry["ionic_staged"]
+    assert set(entry["ionic_staged_ms_per_step"]) == {"4", "6", "8"}
+    batch.set_ionic(0, 0, 0)
     again, t2 = tune_batch(batch, steps=3, cache=cache)
     assert again == choice and t2 is None          # served from the cache
     assert batch.ionic_tiles_per_block == entry["ionic_tiles_per_block"]
+    assert batch.ionic_staged == entry["ionic_staged"]
     batch.run()
     for c, s in zip(cases, sims):
         g = golden(c["name"])

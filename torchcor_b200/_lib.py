@@ -61,7 +61,8 @@ class tcb_batch_plan(C.Structure):
         ("cg_stage_ok", _i32), ("cg_flags", _i32),
         ("group_tiles", _i64 * 3),
         ("total_slices", _i64), ("group_consts", (C.c_char * 1024) * 3),
-        ("ionic_tiles_per_block", _i32), ("ionic_blocks_per_sm", _i32),
+        ("ionic_tiles_per_block", _i32), ("ionic_blocks_per_sm", _i32), ("ionic_staged", _i32),
+        ("ionic_stage_ok", _i32),
     ]
 
 
@@ -105,7 +106,7 @@ SIGNATURES = [
     ("tcb_batch_workspace_bytes", _i64, [_i32]),
     ("tcb_batch_prepare", C.c_int, [C.POINTER(tcb_mono), _i32, _vp, _i64, C.POINTER(tcb_batch_plan)]),
     ("tcb_batch_set_cg", C.c_int, [C.POINTER(tcb_batch_plan), _i32]),
-    ("tcb_batch_set_ionic", C.c_int, [C.POINTER(tcb_batch_plan), _i32, _i32]),
+    ("tcb_batch_set_ionic", C.c_int, [C.POINTER(tcb_batch_plan), _i32, _i32, _i32]),
     ("tcb_batch_run", C.c_int, [C.POINTER(tcb_batch_plan), _i64, _vp]),
     ("tcb_batch_check", C.c_int, [C.POINTER(tcb_batch_plan), _vp]),
 ]

@@ -146,6 +146,14 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
         for (int k = 0; k < 4; ++k)
             if (reinterpret_cast<uintptr_t>(ptrs[k]) % 16 != 0) stage_ok = 0;
     }
+    // the staged ionic form copies per-node rows (n_pad a multiple of 128 floats apart)
+    int ionic_stage_ok = 1;
+    for (int i = 0; i < n && ionic_stage_ok; ++i) {
+        const MonoDev& d = devs[i];
+        const void* ptrs[6] = {d.x, d.state, d.at, d.rt, d.stim_bits, d.bp};
+        for (const void* q : ptrs)
+            if (reinterpret_cast<uintptr_t>(q) % 16 != 0) ionic_stage_ok = 0;
+    }
     Layout L = layout(n);
     if ((int64_t)L.total > bytes) return fail(TCB_ERANGE, "batch workspace too small");
 
@@ -231,6 +239,8 @@ extern "C" int tcb_batch_prepare(const tcb_mono* sims, int32_t n, void* workspac
     plan->total_slices = S;
     plan->ionic_tiles_per_block = 0;
     plan->ionic_blocks_per_sm = 0;
+    plan->ionic_staged = 0;
+    plan->ionic_stage_ok = ionic_stage_ok;
     return TCB_OK;
 }
 
@@ -249,13 +259,18 @@ extern "C" int tcb_batch_set_cg(tcb_batch_plan* plan, int32_t variant) {
     return TCB_OK;
 }
 
-extern "C" int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block, int32_t blocks_per_sm) {
+extern "C" int tcb_batch_set_ionic(tcb_batch_plan* plan, int32_t tiles_per_block, int32_t blocks_per_sm,
+                                   int32_t staged) {
     if (!plan || !plan->workspace || tiles_per_block < 0 || tiles_per_block > kBatchMaxTilesPerBlock)
         return fail(TCB_EINVAL, "tcb_batch_set_ionic: tiles per block outside 0..64");
-    if (!batch_ionic_blocks_ok(blocks_per_sm))
-        return fail(TCB_EINVAL, "tcb_batch_set_ionic: blocks per SM not 0, 4, 6, 8 or 12");
+    if (staged != 0 && staged != 1) return fail(TCB_EINVAL, "tcb_batch_set_ionic: staged not 0 or 1");
+    if (!batch_ionic_blocks_ok(blocks_per_sm, staged))
+        return fail(TCB_EINVAL, "tcb_batch_set_ionic: blocks per SM not 0, 4, 6, 8 or (unstaged) 12");
+    if (staged && !plan->ionic_stage_ok)
+        return fail(TCB_ERANGE, "tcb_batch_set_ionic: staged form needs 16-byte aligned per-node arrays");
     plan->ionic_tiles_per_block = tiles_per_block;
     plan->ionic_blocks_per_sm = blocks_per_sm;
+    plan->ionic_staged = staged;
     return TCB_OK;
 }
 
@@ -266,14 +281,15 @@ extern "C" int tcb_batch_run(const tcb_batch_plan* plan, int64_t steps, void* st
         plan->cg_flags > 7)
         return fail(TCB_EINVAL, "tcb_batch_run: plan CG grid out of range");
     if (plan->ionic_tiles_per_block < 0 || plan->ionic_tiles_per_block > kBatchMaxTilesPerBlock ||
-        !batch_ionic_blocks_ok(plan->ionic_blocks_per_sm))
+        plan->ionic_staged < 0 || plan->ionic_staged > 1 || (plan->ionic_staged && !plan->ionic_stage_ok) ||
+        !batch_ionic_blocks_ok(plan->ionic_blocks_per_sm, plan->ionic_staged))
         return fail(TCB_EINVAL, "tcb_batch_run: plan ionic launch out of range");
     cudaStream_t s = as_stream(stream);
     const BatchWS* W = static_cast<const BatchWS*>(plan->workspace);
     for (int64_t k = 0; k < steps; ++k) {
         int st = launch_batch_ionic_all(W, plan->n_groups, plan->group_model, plan->group_tiles, plan->group_shared,
                                         plan->group_consts, plan->ionic_tiles_per_block,
-                                        plan->ionic_blocks_per_sm, s);
+                                        plan->ionic_blocks_per_sm, plan->ionic_staged, s);
         if (st) return st;
         st = launch_batch_cg(W, plan->cg_blocks, (size_t)plan->cg_smem, plan->cg_variant, plan->cg_stage_bytes,
                              plan->cg_flags, s);

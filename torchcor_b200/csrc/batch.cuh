@@ -58,9 +58,11 @@ struct BatchWS {
 constexpr int kBatchMaxTilesPerBlock = 64;   // tcb_batch_set_ionic's upper limit
 int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* models, const int64_t* tiles,
                            const int32_t* shared, const char (*consts)[1024], int tiles_per_block,
-                           int blocks_per_sm, cudaStream_t s);
+                           int blocks_per_sm, int staged, cudaStream_t s);
 // register budgets of the batched ionic kernel (blocks of 128 threads per SM); 0 = default
-inline bool batch_ionic_blocks_ok(int b) { return b == 0 || b == 4 || b == 6 || b == 8 || b == 12; }
+inline bool batch_ionic_blocks_ok(int b, int staged) {
+    return b == 0 || b == 4 || b == 6 || b == 8 || (b == 12 && !staged);
+}
 // batched CG variants: 1 / 2 = streaming, sized for 1 / 2 blocks per SM;
 // 3 = ELL streams staged in shared memory by bulk copies, 1 block per SM
 // flags: the (int16 columns 4, A rebuilt 2, linear guess 1) combination all the

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include "batch.cuh"
+#include "bulk.cuh"
 #include "ionic_crn.cuh"
 #include "ionic_ms.cuh"
 #include "ionic_node.cuh"
@@ -126,6 +127,183 @@ __global__ void __launch_bounds__(kThreads, MINB) batch_ionic_kernel(const Ionic
     }
 }
 
+// ---------------------------------------------------------------------------
+// Staged form (the plan's ionic_staged): the state rows, u, AT/RT and stimulus
+// bits of a block's next 128-node tile are copied into shared memory by bulk
+// asynchronous copies (cp.async.bulk from this GPU's memory, no multicast,
+// completion counted on an mbarrier, bounded waits) while the block computes the
+// current tile from shared memory, as mono_ionic_staged_kernel does for one
+// simulation.  A block walks a contiguous range of its group's tiles (the launch
+// sizes the grid to the register budget's blocks per SM); the two-stage pipeline
+// runs over each stretch of that range lying in one simulation and restarts at
+// the next.  Padding nodes (n <= i < n_pad) are computed like the others, on
+// memory that exists, and nothing reads their results; their u stays 0, so AT/RT
+// are never set for them, and snapshots are written for real nodes only.  TTP and
+// CRN take the division policy of the single-simulation default (QFast); the
+// Mitchell-Schaeffer group of a staged launch runs the unstaged walk.
+template <bool WITH_CRN>
+struct BatchStage {
+    static constexpr int kMaxStates = WITH_CRN ? (CRN::kStates > TTP::kStates ? CRN::kStates : TTP::kStates)
+                                               : (TTP::kStates > MS::kStates ? TTP::kStates : MS::kStates);
+    static constexpr int kRows = kMaxStates + 4;   // state rows, u, AT, RT, stimulus bits
+    static constexpr size_t kBytes = 2ull * kRows * kBatchTile * sizeof(float);   // both stages
+};
+
+template <class M>
+struct StagedPolicy {
+    using Q = QFast;
+};
+
+// Walks tiles [blk*tpb, +tpb) of group g; false after a timed-out copy wait (the
+// error word is set; the block returns).
+template <class M, bool SHARED, int ROWS>
+__device__ __forceinline__ bool staged_tiles(const BatchWS* __restrict__ W, int g, int tpb, int64_t blk,
+                                             const typename M::C& c0, MonoDev& sd, typename M::Tables& sT,
+                                             int& s_lo, float* stage, uint64_t* bar, uint32_t& phase) {
+    using Q = typename StagedPolicy<M>::Q;
+    constexpr int S = M::kStates, T = kBatchTile;
+    const BatchGroup& G = W->groups[g];
+    const int64_t total_tiles = G.tile_prefix[G.count];
+    const int64_t t0 = blk * tpb;
+    const int64_t t1 = t0 + tpb < total_tiles ? t0 + tpb : total_tiles;
+    const int tid = threadIdx.x;
+    int lo = -1;
+    int64_t tile = t0;
+    while (tile < t1) {
+        // enter the simulation of `tile` (block-uniform)
+        if (lo >= 0) __syncthreads();   // every thread is done with the previous view
+        if (tid == 0) {
+            int l = lo < 0 ? 0 : lo + 1, h = G.count - 1;
+            while (l < h) {
+                const int mid = (l + h + 1) >> 1;
+                if (G.tile_prefix[mid] <= tile) l = mid;
+                else h = mid - 1;
+            }
+            s_lo = l;
+        }
+        __syncthreads();
+        lo = s_lo;
+        {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(W->dev + G.idx[lo]);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+            for (int t = tid; t < (int)(sizeof(MonoDev) / 4); t += blockDim.x) dst[t] = src[t];
+            const uint32_t* ts = reinterpret_cast<const uint32_t*>(static_cast<const typename M::Tables*>(G.tables) + lo);
+            uint32_t* td = reinterpret_cast<uint32_t*>(&sT);
+            for (int t = tid; t < (int)(sizeof(typename M::Tables) / 4); t += blockDim.x) td[t] = ts[t];
+        }
+        const int64_t first = G.tile_prefix[lo];
+        const int64_t end = G.tile_prefix[lo + 1] < t1 ? G.tile_prefix[lo + 1] : t1;
+        __syncthreads();
+        const int64_t step = sd.counter[0];
+        if (step < 1 || step > sd.nt) {   // this simulation does not step now
+            tile = end;
+            continue;
+        }
+        const StepView sv = step_view(sd, step);
+        const typename M::C& c = SHARED ? c0 : static_cast<const typename M::C*>(G.consts)[lo];
+        // thread 0: copy tile t of this simulation into stage st
+        auto issue = [&](int st, int64_t t) {
+            const int64_t i0 = (t - first) * T;
+            float* buf = stage + (size_t)st * ROWS * T;
+            constexpr uint32_t bytes = T * sizeof(float);
+            const uint32_t total = bytes * (S + 1) + (sv.do_atrt ? 2 * bytes : 0) + (sv.smask ? bytes : 0);
+            fence_proxy_async_smem();
+            mbar_arrive_tx(&bar[st], total);
+            for (int k = 0; k < S; ++k) bulk_load(buf + k * T, sd.state + k * sd.n_pad + i0, bytes, &bar[st]);
+            bulk_load(buf + S * T, sv.u + i0, bytes, &bar[st]);
+            if (sv.do_atrt) {
+                bulk_load(buf + (S + 1) * T, sd.at + i0, bytes, &bar[st]);
+                bulk_load(buf + (S + 2) * T, sd.rt + i0, bytes, &bar[st]);
+            }
+            if (sv.smask) bulk_load(buf + (S + 3) * T, sd.stim_bits + i0, bytes, &bar[st]);
+        };
+        if (tid == 0) {
+            issue(0, tile);
+            if (tile + 1 < end) issue(1, tile + 1);
+        }
+        int k = 0;
+        for (int64_t t = tile; t < end; ++t, ++k) {
+            const int st = k & 1;
+            const bool ok = __syncthreads_and(mbar_wait_thread(&bar[st], (phase >> st) & 1u, W->wait.timeout_ns));
+            if (!ok) {
+                // a copy did not complete in time: record it, give the other stage's
+                // copies (issued for the next tile) a bounded wait, and return
+                if (tid == 0) atomicCAS(W->err, 0, TCB_ETIMEOUT);
+                if (t + 1 < end) mbar_wait_thread(&bar[st ^ 1], (phase >> (st ^ 1)) & 1u, W->wait.timeout_ns);
+                return false;
+            }
+            phase ^= 1u << st;
+            const float* buf = stage + (size_t)st * ROWS * T;
+            const int64_t i = (t - first) * T + tid;
+            const float v = buf[S * T + tid];
+            if (sv.do_atrt) {
+                float a = buf[(S + 1) * T + tid];
+                if (v > 0.0f && a == -1.0f) {   // padding nodes keep u = 0 and never pass
+                    a = sv.t_prev;
+                    sd.at[i] = a;
+                }
+                if (a > 0.0f && v < -70.0f && buf[(S + 2) * T + tid] == -1.0f) sd.rt[i] = sv.t_prev;
+            }
+            if (sv.snap && i < sd.n) sv.snap[i] = v;
+            float s[S];
+#pragma unroll
+            for (int q = 0; q < S; ++q) s[q] = buf[q * T + tid];
+            float b = v * sd.cm +
+                      sd.dt * Q::div(M::template step<Q>(v, s, c, sT, M::node_g(c, sd.node_params, sd.n_pad, i)),
+                                     100.0f);
+#pragma unroll
+            for (int q = 0; q < S; ++q) sd.state[q * sd.n_pad + i] = s[q];
+            if (sv.smask) {
+                const uint32_t on = reinterpret_cast<const uint32_t*>(buf + (S + 3) * T)[tid] & sv.smask;
+                if (on) b = b + sd.dt * Q::div(stim_sum(sd, sv.smask, on), 100.0f);
+            }
+            sd.bp[i] = b;
+            __syncthreads();   // every thread is done with this stage
+            if (tid == 0 && t + 2 < end) issue(st, t + 2);
+        }
+        tile = end;
+    }
+    return true;
+}
+
+template <class M, int ROWS>
+__device__ __forceinline__ bool run_group_staged(const IonicLaunch& P, int k, int64_t blk, const typename M::C& c0,
+                                                 MonoDev& sd, unsigned char* tabs, int& s_lo, float* stage,
+                                                 uint64_t* bar, uint32_t& phase) {
+    auto& sT = *reinterpret_cast<typename M::Tables*>(tabs);
+    if (P.shared[k]) return staged_tiles<M, true, ROWS>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo, stage, bar, phase);
+    return staged_tiles<M, false, ROWS>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo, stage, bar, phase);
+}
+
+template <bool WITH_CRN, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) batch_ionic_staged_kernel(const IonicLaunch P) {
+    constexpr int ROWS = BatchStage<WITH_CRN>::kRows;
+    extern __shared__ __align__(128) float stage[];      // [2][ROWS][128]
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ MonoDev sd;
+    __shared__ __align__(16) unsigned char tabs[kTablesBytes];
+    __shared__ int s_lo;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0]);
+        mbar_init(&bar[1]);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    int k = 0;
+    while (k + 1 < P.n_groups && (int64_t)blockIdx.x >= P.block_prefix[k + 1]) ++k;
+    const int64_t blk = (int64_t)blockIdx.x - P.block_prefix[k];
+    switch (P.W->groups[P.group[k]].model) {
+        // Mitchell-Schaeffer's one state and few operations leave nothing for the
+        // stage to hide: its group takes the unstaged walk (short blocks)
+        case TCB_MODEL_MS: run_group<MS>(P, k, blk, P.ms, sd, tabs, s_lo); break;
+        case TCB_MODEL_TTP: run_group_staged<TTP, ROWS>(P, k, blk, P.ttp, sd, tabs, s_lo, stage, bar, phase); break;
+        default:
+            if constexpr (WITH_CRN) run_group_staged<CRN, ROWS>(P, k, blk, P.crn, sd, tabs, s_lo, stage, bar, phase);
+            break;
+    }
+}
+
 }  // namespace
 
 size_t model_consts_bytes(int model) {
@@ -191,6 +369,19 @@ int model_tables_view(int model, const float* tables, const double* params, void
 }
 
 template <bool WITH_CRN>
+int launch_ionic_staged(const IonicLaunch& P, unsigned blocks, int blocks_per_sm, cudaStream_t s) {
+    constexpr size_t smem = BatchStage<WITH_CRN>::kBytes;
+    switch (blocks_per_sm) {
+        case 4: batch_ionic_staged_kernel<WITH_CRN, 4><<<blocks, kThreads, smem, s>>>(P); break;
+        case 6: batch_ionic_staged_kernel<WITH_CRN, 6><<<blocks, kThreads, smem, s>>>(P); break;
+        case 8: batch_ionic_staged_kernel<WITH_CRN, 8><<<blocks, kThreads, smem, s>>>(P); break;
+        default: return fail(TCB_EINVAL, "staged batched ionic kernel: blocks per SM not 4, 6 or 8");
+    }
+    TCB_CHECK_LAUNCH("staged batched ionic kernel");
+    return TCB_OK;
+}
+
+template <bool WITH_CRN>
 int launch_ionic_instance(const IonicLaunch& P, unsigned blocks, int blocks_per_sm, cudaStream_t s) {
     switch (blocks_per_sm) {
         case 4: batch_ionic_kernel<WITH_CRN, 4><<<blocks, kThreads, 0, s>>>(P); break;
@@ -205,7 +396,7 @@ int launch_ionic_instance(const IonicLaunch& P, unsigned blocks, int blocks_per_
 
 int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* models, const int64_t* tiles,
                            const int32_t* shared, const char (*consts)[1024], int tiles_per_block,
-                           int blocks_per_sm, cudaStream_t s) {
+                           int blocks_per_sm, int staged, cudaStream_t s) {
     static_assert(sizeof(IonicLaunch) <= 4000, "kernel argument block");
     IonicLaunch P;
     memset(&P, 0, sizeof P);
@@ -221,12 +412,25 @@ int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* m
     P.n_groups = n;
     bool with_crn = false;
     int64_t blocks = 0;
+    // the staged form's TTP and CRN groups walk contiguous tile ranges, each group
+    // over as many blocks as the register budget keeps resident (the groups run
+    // heavier first, so each fills the GPU in turn); Mitchell-Schaeffer takes the
+    // unstaged walk's short blocks, which fill the slots as the others finish
+    const int staged_bps = blocks_per_sm > 0 ? blocks_per_sm : 6;
     for (int k = 0; k < n; ++k) {
         const int g = order[k];
-        // tiles per block: the plan's choice (a tuning knob), else sized from the group
-        const int64_t per = (tiles[g] + (int64_t)sms * kBlocksPerSmTarget - 1) / ((int64_t)sms * kBlocksPerSmTarget);
-        const int tpb = tiles_per_block > 0 ? tiles_per_block
-                                            : (int)(per < 1 ? 1 : per > kMaxTilesPerBlock ? kMaxTilesPerBlock : per);
+        int tpb;
+        if (tiles_per_block > 0) {   // the plan's choice (a tuning knob)
+            tpb = tiles_per_block;
+        } else if (staged && models[g] != TCB_MODEL_MS) {
+            const int64_t want = (int64_t)sms * staged_bps;
+            const int64_t per = (tiles[g] + want - 1) / want;
+            tpb = (int)(per < 1 ? 1 : per > kBatchMaxTilesPerBlock ? kBatchMaxTilesPerBlock : per);
+        } else {                      // sized from the group
+            const int64_t per =
+                (tiles[g] + (int64_t)sms * kBlocksPerSmTarget - 1) / ((int64_t)sms * kBlocksPerSmTarget);
+            tpb = (int)(per < 1 ? 1 : per > kMaxTilesPerBlock ? kMaxTilesPerBlock : per);
+        }
         P.group[k] = g;
         P.tpb[k] = tpb;
         P.shared[k] = shared[g];
@@ -245,6 +449,10 @@ int launch_batch_ionic_all(const BatchWS* ws_dev, int n_groups, const int32_t* m
     P.block_prefix[n] = blocks;
     if (blocks < 1) return TCB_OK;
     if (blocks > INT32_MAX) return fail(TCB_ERANGE, "batched ionic grid too large");
+    if (staged) {
+        if (with_crn) return launch_ionic_staged<true>(P, (unsigned)blocks, staged_bps, s);
+        return launch_ionic_staged<false>(P, (unsigned)blocks, staged_bps, s);
+    }
     if (with_crn) return launch_ionic_instance<true>(P, (unsigned)blocks, blocks_per_sm > 0 ? blocks_per_sm : 8, s);
     return launch_ionic_instance<false>(P, (unsigned)blocks, blocks_per_sm > 0 ? blocks_per_sm : 12, s);
 }

@@ -33,6 +33,7 @@ class MonodomainBatch:
         self._cg_variant = None
         self._ionic_tpb = 0
         self._ionic_bps = 0
+        self._ionic_staged = 0
 
     def add(self, sim, a_tol=1e-5, r_tol=1e-5, max_iter=100, calculate_AT_RT=True, linear_guess=True,
             snapshot_interval=1):
@@ -68,8 +69,13 @@ class MonodomainBatch:
                 self._cg_variant = None
             else:
                 check(st)
-        if self._ionic_tpb or self._ionic_bps:
-            check(lib.tcb_batch_set_ionic(C.byref(self._plan), int(self._ionic_tpb), int(self._ionic_bps)))
+        if self._ionic_staged and not self._plan.ionic_stage_ok:
+            self._ionic_staged = 0       # the arrays of these simulations do not allow it
+            if self._ionic_bps == 12:
+                self._ionic_bps = 0
+        if self._ionic_tpb or self._ionic_bps or self._ionic_staged:
+            check(lib.tcb_batch_set_ionic(C.byref(self._plan), int(self._ionic_tpb), int(self._ionic_bps),
+                                          int(self._ionic_staged)))
         self._dirty = False
 
     def set_cg(self, variant):
@@ -81,20 +87,34 @@ class MonodomainBatch:
         if self.sims and not self._dirty:
             check(_lib.load().tcb_batch_set_cg(C.byref(self._plan), int(variant)))
 
-    def set_ionic(self, tiles_per_block=None, blocks_per_sm=None):
+    def set_ionic(self, tiles_per_block=None, blocks_per_sm=None, staged=None):
         """The batched ionic launch: tiles of 128 nodes each block walks, 0 (sized
-        from the model groups, the default) or 1..64, and the kernel instance's
-        register budget, 0 (default: 8 blocks of 128 threads per SM with CRN
-        simulations, else 12) or 4, 6, 8, 12.  ``None`` keeps the current value."""
+        from the model groups, the default) or 1..64; the kernel instance's register
+        budget, 0 (default: 8 blocks of 128 threads per SM with CRN simulations, else
+        12; staged 6) or 4, 6, 8, 12 (not 12 staged); and the staged form (each
+        block's next tile copied into shared memory by bulk copies while it computes
+        one; hardware division for TTP and CRN, as the single-simulation default).
+        ``None`` keeps the current value."""
         tpb = self._ionic_tpb if tiles_per_block is None else int(tiles_per_block)
         bps = self._ionic_bps if blocks_per_sm is None else int(blocks_per_sm)
+        stg = self._ionic_staged if staged is None else int(bool(staged))
         if not 0 <= tpb <= 64:
             raise ValueError("tiles_per_block must be in 0..64")
-        if bps not in (0, 4, 6, 8, 12):
-            raise ValueError("blocks_per_sm must be 0, 4, 6, 8 or 12")
-        self._ionic_tpb, self._ionic_bps = tpb, bps
+        if bps not in ((0, 4, 6, 8) if stg else (0, 4, 6, 8, 12)):
+            raise ValueError("blocks_per_sm must be 0, 4, 6, 8 or (unstaged) 12")
+        self._ionic_tpb, self._ionic_bps, self._ionic_staged = tpb, bps, stg
         if self.sims and not self._dirty:
-            check(_lib.load().tcb_batch_set_ionic(C.byref(self._plan), tpb, bps))
+            check(_lib.load().tcb_batch_set_ionic(C.byref(self._plan), tpb, bps, stg))
+
+    @property
+    def ionic_staged(self):
+        return self._ionic_staged
+
+    def ionic_stage_ok(self):
+        """True if the simulations' per-node arrays allow the staged ionic form."""
+        if self._dirty and self.sims:
+            self._prepare()
+        return bool(self._plan.ionic_stage_ok)
 
     @property
     def ionic_tiles_per_block(self):

@@ -88,11 +88,13 @@ def batch_key(device, n_nodes, models) -> str:
 
 BATCH_IONIC_TPB = (0, 1, 2, 4, 8, 16)   # batched ionic tiles per block (0: sized from the groups)
 BATCH_IONIC_BPS = (0, 4, 6, 8, 12)      # its register budget in blocks per SM (0: the default)
+BATCH_IONIC_STAGED_BPS = (4, 6, 8)      # register budgets of the staged form
 
 
 def tune_batch(batch, steps=10, cache=None, force=False):
-    """Pick the batched CG variant, then the batched ionic launch's tiles per block,
-    then its register budget, for ``batch`` (a prepared ``MonodomainBatch``).
+    """Pick the batched CG variant, then the batched ionic launch (tiles per block,
+    then register budget of the unstaged form; the staged form at each of its
+    budgets; the fastest of them), for ``batch`` (a prepared ``MonodomainBatch``).
 
     Uses the cached choice when there is one (unless ``force``); otherwise runs
     ``steps`` real batch steps with each candidate after one untimed step, keeps
@@ -108,10 +110,16 @@ def tune_batch(batch, steps=10, cache=None, force=False):
     if hit is not None:
         if int(hit["cg_variant"]) in batch.cg_variants():
             batch.set_cg(int(hit["cg_variant"]))
-            batch.set_ionic(int(hit.get("ionic_tiles_per_block", 0)), int(hit.get("ionic_blocks_per_sm", 0)))
+            launch = (int(hit.get("ionic_tiles_per_block", 0)), int(hit.get("ionic_blocks_per_sm", 0)),
+                      int(hit.get("ionic_staged", 0)))
+            if launch[2] and not batch.ionic_stage_ok():
+                launch = (0, 0, 0)        # these arrays do not allow the staged form: defaults
+            batch.set_ionic(*launch)
             return int(hit["cg_variant"]), None
     candidates = batch.cg_variants()
-    need = (steps + 1) * (len(candidates) + len(BATCH_IONIC_TPB) + len(BATCH_IONIC_BPS))
+    staged_ok = batch.ionic_stage_ok()
+    need = (steps + 1) * (len(candidates) + len(BATCH_IONIC_TPB) + len(BATCH_IONIC_BPS) +
+                          (len(BATCH_IONIC_STAGED_BPS) if staged_ok else 0))
     if min(s.nt + 1 - s._sim["next_step"] for s in sims) < need:
         return batch.cg_config[0], None
     stream = torch.cuda.current_stream(batch.device)
@@ -134,21 +142,33 @@ def tune_batch(batch, steps=10, cache=None, force=False):
     batch.set_cg(best)
     tpb_times = {}
     for t in BATCH_IONIC_TPB:
-        batch.set_ionic(tiles_per_block=t)
+        batch.set_ionic(tiles_per_block=t, blocks_per_sm=0, staged=0)
         tpb_times[t] = timed()
     tpb = min(tpb_times, key=tpb_times.get)
-    batch.set_ionic(tiles_per_block=tpb)
     bps_times = {}
     for b in BATCH_IONIC_BPS:
-        batch.set_ionic(blocks_per_sm=b)
+        batch.set_ionic(tiles_per_block=tpb, blocks_per_sm=b, staged=0)
         bps_times[b] = timed()
     bps = min(bps_times, key=bps_times.get)
-    batch.set_ionic(blocks_per_sm=bps)
+    staged_times = {}
+    if staged_ok:
+        for b in BATCH_IONIC_STAGED_BPS:
+            batch.set_ionic(tiles_per_block=0, blocks_per_sm=b, staged=1)
+            staged_times[b] = timed()
+    staged = bool(staged_times) and min(staged_times.values()) < bps_times[bps]
+    if staged:
+        sb = min(staged_times, key=staged_times.get)
+        batch.set_ionic(tiles_per_block=0, blocks_per_sm=sb, staged=1)
+        entry_tpb, entry_bps = 0, sb
+    else:
+        batch.set_ionic(tiles_per_block=tpb, blocks_per_sm=bps, staged=0)
+        entry_tpb, entry_bps = tpb, bps
     cache.put(key, {"cg_variant": best, "ms_per_step": {str(k): v for k, v in times.items()},
-                    "ionic_tiles_per_block": tpb,
+                    "ionic_tiles_per_block": entry_tpb, "ionic_blocks_per_sm": entry_bps,
+                    "ionic_staged": int(staged),
                     "ionic_ms_per_step": {str(k): v for k, v in tpb_times.items()},
-                    "ionic_blocks_per_sm": bps,
-                    "ionic_budget_ms_per_step": {str(k): v for k, v in bps_times.items()}})
+                    "ionic_budget_ms_per_step": {str(k): v for k, v in bps_times.items()},
+                    "ionic_staged_ms_per_step": {str(k): v for k, v in staged_times.items()}})
     return best, times
 
 
