@@ -1,13 +1,14 @@
 """Failure detection of the bounded device waits, without a GPU fault.
 
 Every device-side wait (the grid barriers of the persistent CG kernels, the
-mbarriers of the batched kernel's bulk copies) gives up after a time limit,
+mbarriers of the batched kernels' bulk copies) gives up after a time limit,
 records TCB_ETIMEOUT in the simulation's error word and returns, so a lost
 block or copy can never hang the GPU.  The internal test variable
 TCB_TEST_WAIT_STALL makes such a wait run out on purpose (limit 10 ms):
 "grid" makes every grid barrier wait for one arrival more than the grid has,
-"copy" leaves the first bulk copy of the batched kernel's first warp unissued
-while its mbarrier still expects the bytes.  The tests check the reported
+"copy" leaves the first bulk copies of a staged batched kernel (the first warp
+of the batched CG kernel, the first block of the staged batched ionic kernel)
+unissued while their mbarrier still expects the bytes.  The tests check the reported
 status and that the next normal run on the same GPU is correct.
 """
 import ctypes as C
@@ -73,6 +74,27 @@ def test_bulk_copy_wait_timeout_is_reported(lib, cuda, tmp_path, monkeypatch):
     assert 3 in batch.cg_variants()
     batch.set_cg(3)                                        # ELL streams staged by bulk copies
     assert batch.cg_config[0] == 3
+    batch.step(2)
+    with pytest.raises(_lib.TcbError) as e:
+        batch.check()
+    assert e.value.status == _lib.TCB_ETIMEOUT
+    monkeypatch.delenv("TCB_TEST_WAIT_STALL")
+    _clean_solve_matches_reference(case, d, cuda)
+
+
+def test_staged_batched_ionic_copy_wait_timeout_is_reported(lib, cuda, tmp_path, monkeypatch):
+    """The staged batched ionic kernel: block 0's first tile copies are not made while
+    its mbarrier expects the bytes; the bounded wait runs out and is reported."""
+    from torchcor_b200 import _lib
+    from torchcor_b200.simulator import MonodomainBatch
+    case = CS.case("cube8_ttp_f32")
+    d = case_mesh_dir(case, tmp_path)
+    monkeypatch.setenv("TCB_TEST_WAIT_STALL", "copy")     # read when the batch plan is prepared
+    batch = MonodomainBatch(cuda)
+    batch.add(_sim(case, d, cuda), case["tol"], case["tol"], case["max_iter"])
+    batch.set_cg(2)                                        # streaming CG: no copies of its own
+    batch.set_ionic(0, 6, staged=True)
+    assert batch.ionic_staged == 1
     batch.step(2)
     with pytest.raises(_lib.TcbError) as e:
         batch.check()

@@ -159,7 +159,8 @@ struct StagedPolicy {
 template <class M, bool SHARED, int ROWS>
 __device__ __forceinline__ bool staged_tiles(const BatchWS* __restrict__ W, int g, int tpb, int64_t blk,
                                              const typename M::C& c0, MonoDev& sd, typename M::Tables& sT,
-                                             int& s_lo, float* stage, uint64_t* bar, uint32_t& phase) {
+                                             int& s_lo, float* stage, uint64_t* bar, uint32_t& phase,
+                                             uint32_t& drop) {
     using Q = typename StagedPolicy<M>::Q;
     constexpr int S = M::kStates, T = kBatchTile;
     const BatchGroup& G = W->groups[g];
@@ -209,6 +210,10 @@ __device__ __forceinline__ bool staged_tiles(const BatchWS* __restrict__ W, int 
             const uint32_t total = bytes * (S + 1) + (sv.do_atrt ? 2 * bytes : 0) + (sv.smask ? bytes : 0);
             fence_proxy_async_smem();
             mbar_arrive_tx(&bar[st], total);
+            if (drop) {   // test hook: this issue's bytes never arrive, the wait runs out
+                drop = 0;
+                return;
+            }
             for (int k = 0; k < S; ++k) bulk_load(buf + k * T, sd.state + k * sd.n_pad + i0, bytes, &bar[st]);
             bulk_load(buf + S * T, sv.u + i0, bytes, &bar[st]);
             if (sv.do_atrt) {
@@ -269,10 +274,11 @@ __device__ __forceinline__ bool staged_tiles(const BatchWS* __restrict__ W, int 
 template <class M, int ROWS>
 __device__ __forceinline__ bool run_group_staged(const IonicLaunch& P, int k, int64_t blk, const typename M::C& c0,
                                                  MonoDev& sd, unsigned char* tabs, int& s_lo, float* stage,
-                                                 uint64_t* bar, uint32_t& phase) {
+                                                 uint64_t* bar, uint32_t& phase, uint32_t& drop) {
     auto& sT = *reinterpret_cast<typename M::Tables*>(tabs);
-    if (P.shared[k]) return staged_tiles<M, true, ROWS>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo, stage, bar, phase);
-    return staged_tiles<M, false, ROWS>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo, stage, bar, phase);
+    if (P.shared[k])
+        return staged_tiles<M, true, ROWS>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo, stage, bar, phase, drop);
+    return staged_tiles<M, false, ROWS>(P.W, P.group[k], P.tpb[k], blk, c0, sd, sT, s_lo, stage, bar, phase, drop);
 }
 
 template <bool WITH_CRN, int MINB>
@@ -290,6 +296,8 @@ __global__ void __launch_bounds__(kThreads, MINB) batch_ionic_staged_kernel(cons
     }
     __syncthreads();
     uint32_t phase = 0;
+    // test hook (TCB_TEST_WAIT_STALL=copy): block 0's first copies are not made
+    uint32_t drop = (P.W->wait.drop_first_copy && blockIdx.x == 0) ? 1u : 0u;
     int k = 0;
     while (k + 1 < P.n_groups && (int64_t)blockIdx.x >= P.block_prefix[k + 1]) ++k;
     const int64_t blk = (int64_t)blockIdx.x - P.block_prefix[k];
@@ -297,9 +305,10 @@ __global__ void __launch_bounds__(kThreads, MINB) batch_ionic_staged_kernel(cons
         // Mitchell-Schaeffer's one state and few operations leave nothing for the
         // stage to hide: its group takes the unstaged walk (short blocks)
         case TCB_MODEL_MS: run_group<MS>(P, k, blk, P.ms, sd, tabs, s_lo); break;
-        case TCB_MODEL_TTP: run_group_staged<TTP, ROWS>(P, k, blk, P.ttp, sd, tabs, s_lo, stage, bar, phase); break;
+        case TCB_MODEL_TTP: run_group_staged<TTP, ROWS>(P, k, blk, P.ttp, sd, tabs, s_lo, stage, bar, phase, drop); break;
         default:
-            if constexpr (WITH_CRN) run_group_staged<CRN, ROWS>(P, k, blk, P.crn, sd, tabs, s_lo, stage, bar, phase);
+            if constexpr (WITH_CRN)
+                run_group_staged<CRN, ROWS>(P, k, blk, P.crn, sd, tabs, s_lo, stage, bar, phase, drop);
             break;
     }
 }

@@ -18,9 +18,9 @@ constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;  // 2 s: a wait that long 
 // In normal runs: the 2 s timeout and nothing else.  The failure-detection
 // tests set TCB_TEST_WAIT_STALL (wait_limit() in api.cu): then the timeout is
 // 10 ms and either every grid barrier waits for one arrival more than the grid
-// has ("grid") or the first bulk copy of the batched kernel's first warp is not
-// issued while its mbarrier still expects the bytes ("copy"), so that a wait
-// runs out, the error word is set and every block returns.
+// has ("grid") or the first bulk copies of the batched kernels' first warp or
+// block are not made while their mbarrier still expects the bytes ("copy"), so
+// that a wait runs out, the error word is set and every block returns.
 struct WaitLimit {
     uint64_t timeout_ns;
     uint32_t extra_arrivals;
