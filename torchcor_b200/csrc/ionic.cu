@@ -84,26 +84,31 @@ using LaunchFn = int (*)(const MonoDev&, const typename M::C&, const typename M:
 // overlap the arithmetic of the other.  Results go straight to global memory.
 // Blocks never wait for each other; every mbarrier wait is bounded (the error
 // word gets TCB_ETIMEOUT, the block lets its other copies land, then returns).
+// tiles in flight per block: two (three measured slower on B200: TTP 37.5 -> 39.5
+// us a launch at (1,3,fast), the four-blocks-per-SM instances no longer resident)
+#ifndef TCB_IONIC_STAGES
+#define TCB_IONIC_STAGES 2
+#endif
 template <class M, int V>
 struct StagedTile {
+    static constexpr int kStages = TCB_IONIC_STAGES;     // tiles in flight per block
     static constexpr int kTile = kThreads * V;           // nodes per tile
     static constexpr int kRows = M::kStates + 4;         // state rows, u, AT, RT, stimulus bits
-    static constexpr size_t kBytes = 2ull * kRows * kTile * sizeof(float);   // both stages
+    static constexpr size_t kBytes = (size_t)kStages * kRows * kTile * sizeof(float);   // all stages
 };
 
 template <class M, int V, int MINB, class Q>
 __global__ void __launch_bounds__(kThreads, MINB) mono_ionic_staged_kernel(MonoDev d, typename M::C c,
                                                                             typename M::Tables T, int64_t n_tiles) {
     using ST = StagedTile<M, V>;
-    constexpr int S = M::kStates, kTile = ST::kTile, kRows = ST::kRows;
-    extern __shared__ __align__(128) float stage[];      // [2][kRows][kTile]
-    __shared__ __align__(8) uint64_t bar[2];
+    constexpr int S = M::kStates, kTile = ST::kTile, kRows = ST::kRows, NS = ST::kStages;
+    extern __shared__ __align__(128) float stage[];      // [NS][kRows][kTile]
+    __shared__ __align__(8) uint64_t bar[NS];
     const StepView sv = step_view(d, d.counter[0]);
     int32_t* err = d.counter + 1;
     const int tid = threadIdx.x;
     if (tid == 0) {
-        mbar_init(&bar[0]);
-        mbar_init(&bar[1]);
+        for (int st = 0; st < NS; ++st) mbar_init(&bar[st]);
         mbar_init_fence();
     }
     __syncthreads();
@@ -124,20 +129,22 @@ __global__ void __launch_bounds__(kThreads, MINB) mono_ionic_staged_kernel(MonoD
         if (sv.smask) bulk_load(buf + (S + 3) * kTile, d.stim_bits + i0, bytes, &bar[st]);
     };
     const int64_t first = blockIdx.x, stride = gridDim.x;
-    if (tid == 0) {
-        if (first < n_tiles) issue(0, first);
-        if (first + stride < n_tiles) issue(1, first + stride);
-    }
+    if (tid == 0)
+        for (int st = 0; st < NS; ++st)
+            if (first + st * stride < n_tiles) issue(st, first + st * stride);
     uint32_t phase = 0;
     int k = 0;
     for (int64_t tile = first; tile < n_tiles; tile += stride, ++k) {
-        const int st = k & 1;
+        const int st = k % NS;
         const bool ok = __syncthreads_and(mbar_wait_thread(&bar[st], (phase >> st) & 1u, d.wait.timeout_ns));
         if (!ok) {
             // a copy did not complete in time: record it, give the other stage's
             // copies (issued for the next tile) a bounded wait, and return
             if (tid == 0) atomicCAS(err, 0, TCB_ETIMEOUT);
-            if (tile + stride < n_tiles) mbar_wait_thread(&bar[st ^ 1], (phase >> (st ^ 1)) & 1u, d.wait.timeout_ns);
+            for (int j = 1; j < NS; ++j) {   // the other stages hold tiles tile + j*stride
+                const int o = (st + j) % NS;
+                if (tile + j * stride < n_tiles) mbar_wait_thread(&bar[o], (phase >> o) & 1u, d.wait.timeout_ns);
+            }
             return;
         }
         phase ^= 1u << st;
@@ -193,7 +200,7 @@ __global__ void __launch_bounds__(kThreads, MINB) mono_ionic_staged_kernel(MonoD
             st_nodes<V>(d.bp + i0, b);
         }
         __syncthreads();   // every thread is done with this stage
-        if (tid == 0 && tile + 2 * stride < n_tiles) issue(st, tile + 2 * stride);
+        if (tid == 0 && tile + NS * stride < n_tiles) issue(st, tile + NS * stride);
     }
 }
 
