@@ -222,7 +222,7 @@ class Server:
         side = torch.cuda.Stream(self.device)
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0   # noqa: E731
-        tuned = not self.autotune
+        tuned_key = None      # shape of the batch the launch was last chosen for
         self._staged = 0
         # where the loop's time goes: host seconds building, waiting for the round,
         # retiring and joining; device seconds of the batch steps (CUDA events)
@@ -237,9 +237,17 @@ class Server:
                 self.in_use += footprint_bytes(req)
                 self._join(req, self._build(req, now))
                 continue
-            if not tuned and len(self.active) >= 2:
-                self.batch.autotune(steps=5)
-                tuned = True
+            if self.autotune and len(self.active) >= 2:
+                # the batch's shape (node and simulation counts in log2 buckets, model
+                # set) changes as requests join and leave: choose its launch again
+                # (from the cache when this shape was seen before; the timed steps
+                # are real steps of the batch)
+                from torchcor_b200.tune import batch_key
+                key = batch_key(self.device, [s._sim["struct"].n_nodes for s in self.batch.sims],
+                                [s.ionic_model.name for s in self.batch.sims])
+                if key != tuned_key:
+                    self.batch.autotune(steps=5)
+                    tuned_key = key
             k = min(self.round_steps, min(s.nt + 1 - s._sim["next_step"] for s in self.batch.sims))
             t1 = time.perf_counter()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
