@@ -596,6 +596,8 @@ def batch_arm(a, world, rank, local, clk, steps=None):
         from torchcor_b200.tune import tune_batch
         tuned = tune_batch(batch, steps=10)[1]
         torch.cuda.synchronize(dev)
+    if a.batch_ionic != "auto":   # force the batched ionic form (its default budget and tiles)
+        batch.set_ionic(0, 0, staged=a.batch_ionic == "staged")
     cg_cfg = batch.cg_config
     ionic_tpb, ionic_bps, ionic_staged = batch.ionic_tiles_per_block, batch.ionic_blocks_per_sm, batch.ionic_staged
     # the timed steps replay CUDA graphs of G steps, the remainder runs as plain launches
@@ -759,6 +761,8 @@ def main():
     ap.add_argument("--batch-graph-steps", type=int, default=50)
     ap.add_argument("--batch-steps", type=int, default=200, help="timed batch steps in the default line")
     ap.add_argument("--no-plain", action="store_true", help="batch: skip the one-at-a-time comparison")
+    ap.add_argument("--batch-ionic", default="auto", choices=["auto", "unstaged", "staged"],
+                    help="batch: batched ionic form (auto = the tuner's choice)")
     ap.add_argument("--cg-variant", type=int, default=0, choices=[0, 1, 2, 3],
                     help="batch: batched CG variant (1/2 streaming, 3 staged); 0 = autotuned")
     ap.add_argument("--profile-steps", type=int, default=200)
