@@ -1,10 +1,11 @@
 """Parity of the sm_100a kernels with the oracle and the reference goldens.
 
-Tolerances: membrane potential within 1e-3 of the
-reference's range (max |dVm| <= 1e-3 * max |Vm_ref|), activation and
-repolarisation times within one dt, CSR pattern bit-exact.  Element-wise
-ionic arithmetic follows the reference's float32 operation order, so the
-remaining differences come from exp/log/expm1 implementations (a few ulp).
+Tolerances: membrane potential within 1e-3 of the reference's range
+(max |dVm| <= 1e-3 * max |Vm_ref|), activation and repolarisation times
+within one dt, CSR pattern bit-exact.  Element-wise ionic arithmetic follows
+the reference's float32 operation order; the remaining differences come from
+exp/log/expm1 implementations, contracted multiply-adds and, in the default
+instances, hardware division (a few ulp per operation).
 """
 import numpy as np
 import pytest
