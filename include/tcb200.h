@@ -222,7 +222,7 @@ typedef struct tcb_mono {
     int32_t* step_iters;     /* [nt+1] CG iterations of each step */
     int32_t* counter;        /* [4]: next step, error code, 2 spare */
     double* scratch;         /* >= tcb_mono_scratch_doubles() */
-    uint32_t* barrier;       /* [4] grid-barrier words */
+    uint32_t* barrier;       /* [4] grid-barrier words, zeroed, 8-byte aligned */
     /* model parameters (host) */
     const double* params;
     /* per-node model parameters (tcb_model_node_params), n_pad floats per row, or NULL */

@@ -287,6 +287,29 @@ def test_misaligned_tables_rejected_before_any_launch(lib):
     assert lib.tcb_model_tables(model, _lib.ptr(params), fake + 8, None) == _lib.TCB_EINVAL
 
 
+def test_misaligned_barrier_words_rejected_before_any_launch(lib):
+    """The CG kernels' grid barrier keeps its count and generation in one 64-bit
+    word: barrier words that are not 8-byte aligned are refused on the host, before
+    any device access (fake addresses are enough)."""
+    import ctypes
+    from torchcor_b200 import _lib
+    m = _lib.tcb_mono()
+    fake = 1 << 20
+    for name, typ in m._fields_:
+        if typ in (ctypes.c_void_p,) or (isinstance(typ, type) and issubclass(typ, ctypes._Pointer)):
+            ctypes.memmove(ctypes.addressof(m) + getattr(type(m), name).offset,
+                           ctypes.byref(ctypes.c_void_p(fake)), ctypes.sizeof(ctypes.c_void_p))
+    m.n_nodes, m.n_pad, m.n_slices, m.nt, m.model = 100, 128, 4, 10, _lib.MODEL_MS
+    m.max_iter, m.cm, m.dt = 10, 0.01, 0.01
+    m.node_params = None
+    ctypes.memmove(ctypes.addressof(m) + type(m).barrier.offset, ctypes.byref(ctypes.c_void_p(fake + 4)),
+                   ctypes.sizeof(ctypes.c_void_p))
+    assert lib.tcb_mono_run(ctypes.byref(m), 1, 2, None) == _lib.TCB_EINVAL
+    buf = ctypes.create_string_buffer(256)
+    lib.tcb_last_error(buf, 256)
+    assert b"barrier" in buf.value
+
+
 def test_mitchell_schaeffer_constructor_forms(lib):
     """MitchellSchaeffer(device, dtype) (the reference's form, dt from the simulator)
     and MitchellSchaeffer(dt, device=..., dtype=...) give ModifiedMS2v's parameters."""

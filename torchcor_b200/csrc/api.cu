@@ -101,6 +101,8 @@ int validate(const tcb_mono* m) {
         !m->step_stim || !m->step_iters || !m->counter || !m->scratch || !m->barrier || !m->params)
         return fail(TCB_EINVAL, "tcb_mono: null pointer");
     if (m->model != TCB_MODEL_MS && !m->tables) return fail(TCB_EINVAL, "tcb_mono: null tables");
+    // the grid barrier's count and generation are one 64-bit word
+    if ((uintptr_t)m->barrier & 7u) return fail(TCB_EINVAL, "tcb_mono: barrier words not 8-byte aligned");
     // the ionic kernels read table column pairs as 8-byte vectors
     if (m->model != TCB_MODEL_MS && ((uintptr_t)m->tables & 15u))
         return fail(TCB_EINVAL, "tcb_mono: tables not 16-byte aligned");

@@ -33,6 +33,12 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     return v;
 }
 
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ uint64_t globaltimer() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -47,21 +53,25 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Grid-wide barrier with a bounded wait: returns false (and the kernel must
 // return) if any block recorded an error or the wait ran past the timeout.
+// One 64-bit word (bar[0..1], 8-byte aligned): arrivals in the low half, the
+// generation in the high half.  A block's arrival (one atomic add) returns the
+// generation it waits to see change; the last arrival adds 2^32 - gridDim.x,
+// which clears the count and advances the generation in one operation, so no
+// block can arrive at the next barrier before the count is clear.
 __device__ __forceinline__ bool grid_barrier(uint32_t* bar, int32_t* err, const WaitLimit& w) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int good = 1;
-        const unsigned gen = ld_acquire(bar + 1);
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1 + w.extra_arrivals) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
+        unsigned long long* word = reinterpret_cast<unsigned long long*>(bar);
+        __threadfence();   // this block's writes before its arrival
+        const unsigned long long old = atomicAdd(word, 1ull);
+        const unsigned gen = (unsigned)(old >> 32);
+        if ((unsigned)old == gridDim.x - 1 + w.extra_arrivals) {
+            atomicAdd(word, (1ull << 32) - (unsigned long long)gridDim.x);
         } else {
             const uint64_t t0 = globaltimer();
-            while (ld_acquire(bar + 1) == gen) {
+            while ((unsigned)(ld_acquire64(word) >> 32) == gen) {
                 if (*(volatile int32_t*)err != 0) {
                     good = 0;
                     break;
